@@ -1,0 +1,113 @@
+"""ctypes bindings of the C ABI declared in ``include/dfjk.h``.
+
+The library ``libdfjk.so`` is built in-tree by ``dftax_b200.build``. There is
+no fallback: if the library is missing or fails to load, every entry point
+raises :class:`LibraryNotLoaded`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, byref, c_char_p, c_double, c_int, c_int32, c_int64, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdfjk.so")
+
+DFJK_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CUDA", 4: "MEMORY", 5: "NUMERIC",
+                6: "STATE"}
+DFJK_FP64 = 0
+DFJK_MIXED = 1
+
+# every symbol include/dfjk.h declares
+EXPORTS = (
+    "dfjk_default_options", "dfjk_create", "dfjk_destroy", "dfjk_last_error",
+    "dfjk_plan_create", "dfjk_plan_destroy", "dfjk_plan_get_info", "dfjk_build", "dfjk_jk",
+    "dfjk_jk_host", "dfjk_energy", "dfjk_eri3c_dense", "dfjk_eri2c_dense", "dfjk_metric_pinv",
+    "dfjk_kept_pairs", "dfjk_boys",
+)
+
+
+class LibraryNotLoaded(RuntimeError):
+    pass
+
+
+class DfjkError(RuntimeError):
+    """A non-OK dfjk_status, with the library's last error message."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.status_name = STATUS_NAMES.get(status, str(status))
+        super().__init__(f"dfjk {self.status_name}: {message}")
+
+
+class Basis(ctypes.Structure):
+    _fields_ = [("ncart", c_int64), ("max_prim", c_int32), ("nsph", c_int32),
+                ("centers", c_void_p), ("exponents", c_void_p), ("coefficients", c_void_p),
+                ("angular", c_void_p), ("cart2sph", c_void_p)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("screen", c_double), ("metric_cutoff", c_double), ("precision", c_int32),
+                ("reserved", c_int32), ("chunk_bytes", c_int64)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("nao", c_int64), ("naux", c_int64), ("nao_cart", c_int64),
+                ("naux_cart", c_int64), ("nshell", c_int64), ("naux_shell", c_int64),
+                ("npair_shell", c_int64), ("nrows", c_int64), ("nfit", c_int64),
+                ("b_bytes", c_int64), ("built", c_int32), ("precision", c_int32)]
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load (once) and return the ctypes library with argtypes set."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or os.environ.get("DFJK_LIB", LIB_PATH)
+    if not os.path.exists(p):
+        raise LibraryNotLoaded(f"{p} not found; build it with `python -m dftax_b200.build`")
+    try:
+        lib = ctypes.CDLL(p)
+    except OSError as e:  # pragma: no cover - depends on the environment
+        raise LibraryNotLoaded(f"cannot load {p}: {e}") from e
+    V, P = c_void_p, POINTER
+    sig = {
+        "dfjk_default_options": (None, [P(Options)]),
+        "dfjk_create": (c_int, [c_int, P(c_void_p)]),
+        "dfjk_destroy": (c_int, [V]),
+        "dfjk_last_error": (c_char_p, [V]),
+        "dfjk_plan_create": (c_int, [V, P(Basis), P(Basis), P(Options), P(c_void_p)]),
+        "dfjk_plan_destroy": (c_int, [V]),
+        "dfjk_plan_get_info": (c_int, [V, P(PlanInfo)]),
+        "dfjk_build": (c_int, [V, V]),
+        "dfjk_jk": (c_int, [V, V, V, c_int64, V, V, V]),
+        "dfjk_jk_host": (c_int, [V, V, V, c_int64, V, V, V]),
+        "dfjk_energy": (c_int, [V, V, c_int32, c_double, P(c_double), V, V]),
+        "dfjk_eri3c_dense": (c_int, [V, V, V]),
+        "dfjk_eri2c_dense": (c_int, [V, V, V]),
+        "dfjk_metric_pinv": (c_int, [V, V, V]),
+        "dfjk_kept_pairs": (c_int, [V, V]),
+        "dfjk_boys": (c_int, [V, V, c_int64, c_int32, V, V]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int, ctx=None):
+    if status != DFJK_OK:
+        lib = load()
+        msg = lib.dfjk_last_error(ctx).decode() if ctx else ""
+        raise DfjkError(status, msg)
+
+
+__all__ = ["load", "check", "Basis", "Options", "PlanInfo", "DfjkError", "LibraryNotLoaded",
+           "EXPORTS", "DFJK_FP64", "DFJK_MIXED", "byref"]

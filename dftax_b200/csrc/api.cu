@@ -1,0 +1,841 @@
+// Host side of the dfjk library: context, plan (shells, screening, layouts),
+// build (metric factor, 3-center rows, B) and the C ABI entry points.
+#include "internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <numeric>
+
+namespace dfjk {
+
+void fail(dfjk_status code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  throw Error{code, buf};
+}
+
+void DevBuf::alloc(size_t n) {
+  free();
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    cudaGetLastError();
+    fail(DFJK_ERR_MEMORY, "cudaMalloc of %zu bytes failed: %s", n, cudaGetErrorString(e));
+  }
+  bytes = n;
+}
+
+void DevBuf::free() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Basis parsing and validation
+// ---------------------------------------------------------------------------
+
+static int comp_index(int l, int lx, int ly) {
+  int idx = 0;
+  for (int x = l; x > lx; --x) idx += l - x + 1;
+  return idx + (l - lx - ly);
+}
+
+// Real solid harmonics r^l Y_lm (unit-sphere normalized, m = -l..l) as an
+// ncart(l) x (2l+1) block in dftax's cartesian order; identity for l <= 1.
+// Closed form of Helgaker, Jorgensen & Olsen, eqs. 6.4.47-6.4.50.
+void standard_block(int l, std::vector<double>& out) {
+  const int nc = ncart(l), ns = 2 * l + 1;
+  out.assign((size_t)nc * ns, 0.0);
+  if (l <= 1) {
+    for (int i = 0; i < ns; ++i) out[i * ns + i] = 1.0;
+    return;
+  }
+  auto fact = [](int n) { double r = 1; for (int i = 2; i <= n; ++i) r *= i; return r; };
+  auto binom = [](int n, int k) {
+    if (k < 0 || k > n) return 0.0;
+    double r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r;
+  };
+  for (int col = 0; col < ns; ++col) {
+    const int m = col - l, am = std::abs(m), vm2 = m < 0 ? 1 : 0;
+    const double nrm = std::sqrt(2.0 * fact(l + am) * fact(l - am) / (m == 0 ? 2.0 : 1.0)) /
+                       (std::pow(2.0, am) * fact(l));
+    for (int t = 0; t <= (l - am) / 2; ++t)
+      for (int u = 0; u <= t; ++u) {
+        const int vmax2 = 2 * ((am - vm2) / 2) + vm2;
+        for (int tv = vm2; tv <= vmax2; tv += 2) {
+          const double sign = ((t + (tv - vm2) / 2) % 2) ? -1.0 : 1.0;
+          const double c = sign * std::pow(0.25, t) * binom(l, t) * binom(l - t, am + t) *
+                           binom(t, u) * binom(am, tv);
+          const int py = 2 * u + tv, px = 2 * t + am - 2 * u - tv, pz = l - 2 * t - am;
+          out[comp_index(l, px, py) * ns + col] += c * nrm;
+        }
+      }
+  }
+  const double scale = std::sqrt((2 * l + 1) / (4.0 * M_PI));
+  for (double& v : out) v *= scale;
+}
+
+// Laplacian of every column polynomial must vanish (harmonic components).
+static bool harmonic(int l, const double* blk, int ns) {
+  if (l <= 1) return true;
+  double big = 0.0;
+  for (int i = 0; i < ncart(l) * ns; ++i) big = std::max(big, std::fabs(blk[i]));
+  const int nlow = ncart(l - 2);
+  for (int col = 0; col < ns; ++col) {
+    std::vector<double> lap(nlow, 0.0);
+    for (int lx = l; lx >= 0; --lx)
+      for (int ly = l - lx; ly >= 0; --ly) {
+        const int lz = l - lx - ly;
+        const double c = blk[comp_index(l, lx, ly) * ns + col];
+        if (c == 0.0) continue;
+        if (lx >= 2) lap[comp_index(l - 2, lx - 2, ly)] += c * lx * (lx - 1);
+        if (ly >= 2) lap[comp_index(l - 2, lx, ly - 2)] += c * ly * (ly - 1);
+        if (lz >= 2) lap[comp_index(l - 2, lx, ly)] += c * lz * (lz - 1);
+      }
+    for (double v : lap)
+      if (std::fabs(v) > 1e-9 * std::max(big, 1.0)) return false;
+  }
+  return true;
+}
+
+// Shells from static metadata (dftax/integrals/eri3c_bucketed.py:119-137):
+// a shell starts where the component sequence restarts at (l, 0, 0).
+static void parse_basis(const dfjk_basis* b, const char* what, int lmax_supported,
+                        bool need_harmonic, Shells& sh, Blocks& blk) {
+  if (!b || !b->centers || !b->exponents || !b->coefficients || !b->angular)
+    fail(DFJK_ERR_INVALID, "%s basis: null array", what);
+  if (b->ncart <= 0 || b->max_prim <= 0)
+    fail(DFJK_ERR_INVALID, "%s basis: ncart=%lld max_prim=%d", what, (long long)b->ncart, b->max_prim);
+  const int64_t n = b->ncart;
+  const int mp = b->max_prim;
+  for (int64_t i = 0; i < n * 3; ++i)
+    if (!std::isfinite(b->centers[i])) fail(DFJK_ERR_NUMERIC, "%s basis: non-finite center", what);
+  for (int64_t i = 0; i < n * mp; ++i)
+    if (!std::isfinite(b->exponents[i]) || !std::isfinite(b->coefficients[i]))
+      fail(DFJK_ERR_NUMERIC, "%s basis: non-finite exponent or coefficient", what);
+  std::vector<int64_t> starts;
+  for (int64_t i = 0; i < n; ++i) {
+    const int* a = b->angular + 3 * i;
+    if (a[0] < 0 || a[1] < 0 || a[2] < 0) fail(DFJK_ERR_INVALID, "%s basis: negative power", what);
+    const int l = a[0] + a[1] + a[2];
+    if (a[0] == l && a[1] == 0 && a[2] == 0) starts.push_back(i);
+  }
+  if (starts.empty() || starts[0] != 0)
+    fail(DFJK_ERR_INVALID, "%s basis rows do not start shells at (l,0,0)", what);
+  starts.push_back(n);
+  sh.reset();
+  sh.n = (int)starts.size() - 1;
+  sh.spherical = b->cart2sph != nullptr;
+  int out = 0;
+  for (int s = 0; s < sh.n; ++s) {
+    const int64_t r0 = starts[s], r1 = starts[s + 1];
+    const int* a0 = b->angular + 3 * r0;
+    const int l = a0[0] + a0[1] + a0[2];
+    if (l > lmax_supported)
+      fail(DFJK_ERR_UNSUPPORTED, "%s basis: angular momentum l=%d exceeds the compiled l<=%d",
+           what, l, lmax_supported);
+    if (r1 - r0 != ncart(l))
+      fail(DFJK_ERR_INVALID, "%s basis: shell at row %lld has %lld rows, expected %d", what,
+           (long long)r0, (long long)(r1 - r0), ncart(l));
+    // canonical component order and uniform per-shell data
+    for (int k = 0; k < ncart(l); ++k) {
+      const int* ak = b->angular + 3 * (r0 + k);
+      int lx = l, kk = k;
+      while (kk > l - lx) { kk -= (l - lx + 1); --lx; }
+      const int ly = (l - lx) - kk;
+      if (ak[0] != lx || ak[1] != ly || ak[2] != l - lx - ly)
+        fail(DFJK_ERR_INVALID, "%s basis: shell at row %lld is not in (lx desc, ly desc) order",
+             what, (long long)r0);
+      for (int d = 0; d < 3; ++d)
+        if (b->centers[3 * (r0 + k) + d] != b->centers[3 * r0 + d])
+          fail(DFJK_ERR_INVALID, "%s basis: components of one shell on different centers", what);
+      for (int q = 0; q < mp; ++q) {
+        if (b->exponents[(r0 + k) * mp + q] != b->exponents[r0 * mp + q])
+          fail(DFJK_ERR_INVALID, "%s basis: components of one shell with different exponents", what);
+        const double c0 = b->coefficients[r0 * mp + q], ck = b->coefficients[(r0 + k) * mp + q];
+        if (std::fabs(ck - c0) > 1e-13 * std::fabs(c0))
+          fail(DFJK_ERR_UNSUPPORTED,
+               "%s basis: per-component coefficients differ within the shell at row %lld", what,
+               (long long)r0);
+      }
+    }
+    int np = 0;
+    for (int q = 0; q < mp; ++q)
+      if (b->exponents[r0 * mp + q] != 0.0) ++np;
+    if (np == 0) fail(DFJK_ERR_INVALID, "%s basis: shell at row %lld has no primitive", what, (long long)r0);
+    sh.l.push_back(l);
+    sh.nprim.push_back(np);
+    sh.prim0.push_back((int)sh.pexp.size());
+    sh.row0.push_back((int)r0);
+    sh.ncomp.push_back(ncart(l));
+    sh.out0.push_back(out);
+    out += sh.spherical ? 2 * l + 1 : ncart(l);
+    for (int d = 0; d < 3; ++d) sh.cen.push_back(b->centers[3 * r0 + d]);
+    for (int q = 0; q < mp; ++q)
+      if (b->exponents[r0 * mp + q] != 0.0) {
+        if (!(b->exponents[r0 * mp + q] > 0.0))
+          fail(DFJK_ERR_INVALID, "%s basis: non-positive exponent", what);
+        sh.pexp.push_back(b->exponents[r0 * mp + q]);
+        sh.pcoef.push_back(b->coefficients[r0 * mp + q]);
+      }
+    sh.lmax = std::max(sh.lmax, l);
+  }
+  sh.ncart = (int)n;
+  sh.nout = out;
+  // transformation blocks (eri3c_bucketed.py:186-218): block diagonal, one per l
+  blk.reset();
+  int off = 0;
+  std::vector<int> have(8, 0);
+  for (int l = 0; l <= 7; ++l) blk.off[l] = 0;
+  std::vector<std::vector<double>> per_l(8);
+  if (!sh.spherical) {
+    if (sh.lmax >= 2)
+      fail(DFJK_ERR_UNSUPPORTED, "%s basis: cartesian shells with l>=2 are not supported "
+           "(pass cart2sph)", what);
+    for (int l = 0; l <= sh.lmax; ++l) standard_block(l, per_l[l]);
+  } else {
+    if (b->nsph <= 0) fail(DFJK_ERR_INVALID, "%s basis: nsph=%d with cart2sph", what, b->nsph);
+    if (b->nsph != sh.nout)
+      fail(DFJK_ERR_INVALID, "%s basis: cart2sph has %d columns, shells need %d", what, b->nsph, sh.nout);
+    const double* C = b->cart2sph;
+    const int ns = b->nsph;
+    for (int s = 0; s < sh.n; ++s) {
+      const int l = sh.l[s], nc = ncart(l), no = 2 * l + 1, r0 = sh.row0[s], c0 = sh.out0[s];
+      double rows = 0.0, inb = 0.0;
+      std::vector<double> blkv((size_t)nc * no);
+      for (int i = 0; i < nc; ++i) {
+        for (int j = 0; j < ns; ++j) rows += std::fabs(C[(int64_t)(r0 + i) * ns + j]);
+        for (int j = 0; j < no; ++j) {
+          const double v = C[(int64_t)(r0 + i) * ns + c0 + j];
+          blkv[i * no + j] = v;
+          inb += std::fabs(v);
+        }
+      }
+      if (std::fabs(rows - inb) > 1e-12 * std::max(1.0, rows))
+        fail(DFJK_ERR_INVALID, "%s cart2sph is not block diagonal over shells (shell l=%d at row %d)",
+             what, l, r0);
+      if (have[l]) {
+        for (size_t q = 0; q < blkv.size(); ++q)
+          if (blkv[q] != per_l[l][q])
+            fail(DFJK_ERR_INVALID, "%s cart2sph blocks differ between shells of l=%d", what, l);
+      } else {
+        per_l[l] = blkv;
+        have[l] = 1;
+        if (need_harmonic && !harmonic(l, blkv.data(), no))
+          fail(DFJK_ERR_UNSUPPORTED, "%s cart2sph block for l=%d is not harmonic", what, l);
+      }
+    }
+  }
+  for (int l = 0; l <= sh.lmax; ++l) {
+    blk.off[l] = off;
+    if (per_l[l].empty()) standard_block(l, per_l[l]);
+    blk.host.insert(blk.host.end(), per_l[l].begin(), per_l[l].end());
+    off += (int)per_l[l].size();
+  }
+  upload(blk.dev, blk.host);
+  upload(sh.d_l, sh.l);
+  upload(sh.d_nprim, sh.nprim);
+  upload(sh.d_prim0, sh.prim0);
+  upload(sh.d_cen, sh.cen);
+  upload(sh.d_pexp, sh.pexp);
+  upload(sh.d_pcoef, sh.pcoef);
+}
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+
+static void make_plan(Plan& p, const dfjk_basis* orb, const dfjk_basis* aux) {
+  parse_basis(orb, "orbital", kLmaxOrb, false, p.orb, p.c2s_orb);
+  parse_basis(aux, "auxiliary", kLmaxAux, true, p.aux, p.c2s_aux);
+  p.nao = p.orb.nout;
+  p.naux = p.aux.nout;
+  const int ns = p.orb.n;
+  // bra shell pairs ia <= ib, optionally Schwarz screened
+  std::vector<int> pa, pb;
+  for (int i = 0; i < ns; ++i)
+    for (int j = i; j < ns; ++j) {
+      pa.push_back(i);
+      pb.push_back(j);
+    }
+  if (p.opts.screen > 0.0) {
+    std::vector<double> q;
+    launch_schwarz(*p.ctx, p.orb, pa, pb, q);
+    double qmax = 0.0;
+    for (double v : q) qmax = std::max(qmax, v);
+    std::vector<int> ka, kb;
+    for (size_t i = 0; i < q.size(); ++i)
+      if (q[i] >= p.opts.screen * qmax) {
+        ka.push_back(pa[i]);
+        kb.push_back(pb[i]);
+      }
+    pa.swap(ka);
+    pb.swap(kb);
+  }
+  // canonical orientation (larger l first) and class buckets
+  struct PR { int l1, l2, s1, s2, a, b; };
+  std::vector<PR> prs;
+  prs.reserve(pa.size());
+  for (size_t i = 0; i < pa.size(); ++i) {
+    int a = pa[i], b = pb[i], s1 = a, s2 = b;
+    if (p.orb.l[a] < p.orb.l[b]) std::swap(s1, s2);
+    prs.push_back({p.orb.l[s1], p.orb.l[s2], s1, s2, a, b});
+  }
+  std::stable_sort(prs.begin(), prs.end(), [](const PR& x, const PR& y) {
+    return x.l1 != y.l1 ? x.l1 < y.l1 : x.l2 < y.l2;
+  });
+  p.classes.clear();
+  p.pair_s1.clear(); p.pair_s2.clear(); p.pair_orig_a.clear(); p.pair_orig_b.clear();
+  p.pair_row0.clear(); p.pair_pp0.clear(); p.pair_npp.clear();
+  std::vector<int> pp_pair, pp_pa, pp_pb;
+  int64_t row = 0, pp = 0, esph = 0;
+  for (size_t i = 0; i < prs.size(); ++i) {
+    const PR& r = prs[i];
+    if (p.classes.empty() || p.classes.back().l1 != r.l1 || p.classes.back().l2 != r.l2) {
+      ClassRange c{r.l1, r.l2, (int64_t)i, 0, pp, 0, esph};
+      p.classes.push_back(c);
+    }
+    ClassRange& c = p.classes.back();
+    c.count++;
+    p.pair_s1.push_back(r.s1);
+    p.pair_s2.push_back(r.s2);
+    p.pair_orig_a.push_back(r.a);
+    p.pair_orig_b.push_back(r.b);
+    p.pair_row0.push_back(row);
+    p.pair_pp0.push_back(pp);
+    const int n1 = p.orb.nprim[r.s1], n2 = p.orb.nprim[r.s2];
+    p.pair_npp.push_back(n1 * n2);
+    for (int x = 0; x < n1; ++x)
+      for (int y = 0; y < n2; ++y) {
+        pp_pair.push_back((int)i);
+        pp_pa.push_back(x);
+        pp_pb.push_back(y);
+      }
+    pp += n1 * n2;
+    c.pp_count += n1 * n2;
+    const int na = 2 * r.l1 + 1, nb = 2 * r.l2 + 1;
+    const int nh = (r.l1 + r.l2 + 1) * (r.l1 + r.l2 + 2) * (r.l1 + r.l2 + 3) / 6;
+    esph += (int64_t)n1 * n2 * na * nb * nh;
+    row += na * nb;
+  }
+  p.nrows = row;
+  p.npp = pp;
+  p.esph_doubles = esph;
+  // rows -> (m, n), kinds, and K lists
+  std::vector<int> rm(row), rn(row);
+  std::vector<int8_t> kind(row);
+  std::vector<int> cnt(p.nao + 1, 0);
+  for (size_t i = 0; i < prs.size(); ++i) {
+    const int s1 = p.pair_s1[i], s2 = p.pair_s2[i];
+    const int na = 2 * p.orb.l[s1] + 1, nb = 2 * p.orb.l[s2] + 1;
+    for (int x = 0; x < na; ++x)
+      for (int y = 0; y < nb; ++y) {
+        const int64_t r = p.pair_row0[i] + x * nb + y;
+        const int m = p.orb.out0[s1] + x, n = p.orb.out0[s2] + y;
+        rm[r] = m;
+        rn[r] = n;
+        kind[r] = (s1 == s2) ? (m >= n ? 1 : 0) : 2;
+        cnt[m + 1]++;
+        if (kind[r] == 2) cnt[n + 1]++;
+      }
+  }
+  for (int m = 0; m < p.nao; ++m) cnt[m + 1] += cnt[m];
+  std::vector<int> krow(cnt[p.nao]), kn(cnt[p.nao]), fill(cnt.begin(), cnt.end() - 1);
+  for (int64_t r = 0; r < row; ++r) {
+    krow[fill[rm[r]]] = (int)r;
+    kn[fill[rm[r]]++] = rn[r];
+    if (kind[r] == 2) {
+      krow[fill[rn[r]]] = (int)r;
+      kn[fill[rn[r]]++] = rm[r];
+    }
+  }
+  // aux columns: shells sorted by l (stable), column runs per l
+  p.aux_order.resize(p.aux.n);
+  std::iota(p.aux_order.begin(), p.aux_order.end(), 0);
+  std::stable_sort(p.aux_order.begin(), p.aux_order.end(),
+                   [&](int x, int y) { return p.aux.l[x] < p.aux.l[y]; });
+  p.aux_col0.assign(p.aux.n, 0);
+  p.aux_perm.assign(p.naux, 0);
+  for (int l = 0; l < 8; ++l) { p.aux_lbegin[l] = 0; p.aux_lcount[l] = 0; }
+  int col = 0;
+  for (int pos = 0; pos < p.aux.n; ++pos) {
+    const int s = p.aux_order[pos], l = p.aux.l[s];
+    if (p.aux_lcount[l] == 0) p.aux_lbegin[l] = pos;
+    p.aux_lcount[l]++;
+    p.aux_col0[s] = col;
+    for (int k = 0; k < 2 * l + 1; ++k) p.aux_perm[col + k] = p.aux.out0[s] + k;
+    col += 2 * l + 1;
+  }
+  // upload
+  upload(p.d_pair_s1, p.pair_s1);
+  upload(p.d_pair_s2, p.pair_s2);
+  upload(p.d_pair_row0, p.pair_row0);
+  upload(p.d_pair_pp0, p.pair_pp0);
+  upload(p.d_pair_npp, p.pair_npp);
+  upload(p.d_pp_pair, pp_pair);
+  upload(p.d_pp_pa, pp_pa);
+  upload(p.d_pp_pb, pp_pb);
+  p.d_pp_P.alloc(std::max<int64_t>(pp, 1) * 3 * sizeof(double));
+  p.d_pp_g.alloc(std::max<int64_t>(pp, 1) * sizeof(double));
+  p.d_pp_pref.alloc(std::max<int64_t>(pp, 1) * sizeof(double));
+  p.d_esph.alloc(std::max<int64_t>(esph, 1) * sizeof(double));
+  upload(p.d_aux_sorted, p.aux_order);
+  upload(p.d_aux_perm, p.aux_perm);
+  upload(p.d_row_m, rm);
+  upload(p.d_row_n, rn);
+  upload(p.d_row_w, kind);
+  upload(p.d_kptr, cnt);
+  upload(p.d_krow, krow);
+  upload(p.d_kn, kn);
+  DFJK_CUDA(cudaDeviceSynchronize());
+}
+
+// ---------------------------------------------------------------------------
+// Build: metric factor, primitive pairs, 3-center rows, B
+// ---------------------------------------------------------------------------
+
+__global__ void scale_factor_kernel(const double* __restrict__ U, const double* __restrict__ w,
+                                    int64_t naux, int64_t k0, int64_t nfit, int64_t ldb,
+                                    double* __restrict__ L) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= naux * ldb) return;
+  const int64_t col = i / naux, r = i % naux;
+  L[i] = col < nfit ? U[(k0 + col) * naux + r] / sqrt(w[k0 + col]) : 0.0;
+}
+
+__global__ void finite_check_kernel(const double* __restrict__ x, int64_t n, int* __restrict__ bad) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n && !isfinite(x[i])) atomicExch(bad, 1);
+}
+
+void check_finite(const double* x, int64_t n, cudaStream_t s, const char* what) {
+  DevBuf flag;
+  flag.alloc(sizeof(int));
+  DFJK_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+  if (n > 0) {
+    finite_check_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, n, flag.as<int>());
+    DFJK_CUDA(cudaGetLastError());
+  }
+  int h = 0;
+  DFJK_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  if (h) fail(DFJK_ERR_NUMERIC, "non-finite values in %s", what);
+}
+
+static int64_t chunk_budget(const Plan& p) {
+  return p.opts.chunk_bytes > 0 ? p.opts.chunk_bytes : (int64_t)2 << 30;
+}
+
+void compute_metric_factor(Plan& p, cudaStream_t s) {
+  Context& c = *p.ctx;
+  const int64_t n = p.naux;
+  p.d_metric.alloc((size_t)n * n * sizeof(double));
+  DFJK_CUDA(cudaMemsetAsync(p.d_metric.p, 0, (size_t)n * n * sizeof(double), s));
+  launch_eri2c(p, p.d_metric.as<double>(), n, s);
+  check_finite(p.d_metric.as<double>(), n * n, s, "the (P|Q) metric");
+  p.d_w.alloc(n * sizeof(double));
+  DFJK_CUSOLVER(cusolverDnSetStream(c.cusolver, s));
+  int lwork = 0;
+  DFJK_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR,
+                                            CUBLAS_FILL_MODE_LOWER, (int)n, p.d_metric.as<double>(),
+                                            (int)n, p.d_w.as<double>(), &lwork));
+  DevBuf work, info;
+  work.alloc((size_t)std::max(lwork, 1) * sizeof(double));
+  info.alloc(sizeof(int));
+  DFJK_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                 (int)n, p.d_metric.as<double>(), (int)n, p.d_w.as<double>(),
+                                 work.as<double>(), lwork, info.as<int>()));
+  int hinfo = 0;
+  p.w_host.resize(n);
+  DFJK_CUDA(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaMemcpyAsync(p.w_host.data(), p.d_w.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  if (hinfo != 0) fail(DFJK_ERR_NUMERIC, "metric eigensolver failed (info=%d)", hinfo);
+  // keep w > cutoff * w_max (dftax/ks/terms.py:191); w ascending -> kept set is a suffix
+  const double thr = p.opts.metric_cutoff * p.w_host[n - 1];
+  int64_t k0 = 0;
+  while (k0 < n && !(p.w_host[k0] > thr)) ++k0;
+  p.k0 = k0;
+  p.nfit = n - k0;
+  if (p.nfit <= 0) fail(DFJK_ERR_NUMERIC, "metric has no eigenvalue above the cutoff");
+  p.ldb = (p.nfit + 7) / 8 * 8;
+  p.d_L.alloc((size_t)n * p.ldb * sizeof(double));
+  const int64_t tot = n * p.ldb;
+  scale_factor_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
+      p.d_metric.as<double>(), p.d_w.as<double>(), n, k0, p.nfit, p.ldb, p.d_L.as<double>());
+  DFJK_CUDA(cudaGetLastError());
+}
+
+// Pair chunks of at most `budget` bytes of raw rows (ld doubles each).
+static std::vector<std::pair<int64_t, int64_t>> pair_chunks(const Plan& p, int64_t ld, int64_t budget) {
+  std::vector<std::pair<int64_t, int64_t>> out;
+  const int64_t npair = (int64_t)p.pair_s1.size();
+  const int64_t max_rows = std::max<int64_t>(budget / (ld * (int64_t)sizeof(double)), 49);
+  int64_t b = 0;
+  while (b < npair) {
+    int64_t e = b;
+    while (e < npair) {
+      const int64_t end_row = (e + 1 < npair) ? p.pair_row0[e + 1] : p.nrows;
+      if (end_row - p.pair_row0[b] > max_rows && e > b) break;
+      ++e;
+    }
+    out.push_back({b, e});
+    b = e;
+  }
+  return out;
+}
+
+static int64_t rows_of(const Plan& p, int64_t b, int64_t e) {
+  const int64_t npair = (int64_t)p.pair_s1.size();
+  const int64_t end_row = e < npair ? p.pair_row0[e] : p.nrows;
+  return end_row - p.pair_row0[b];
+}
+
+void build(Plan& p, cudaStream_t s) {
+  Context& c = *p.ctx;
+  p.built = 0;
+  compute_metric_factor(p, s);
+  launch_pair_setup(p, s);
+  p.d_B.alloc((size_t)std::max<int64_t>(p.nrows, 1) * p.ldb * sizeof(double));
+  const int64_t ld = p.naux;
+  auto chunks = pair_chunks(p, ld, chunk_budget(p));
+  int64_t maxrows = 1;
+  for (auto& ch : chunks) maxrows = std::max(maxrows, rows_of(p, ch.first, ch.second));
+  DevBuf raw;
+  raw.alloc((size_t)maxrows * ld * sizeof(double));
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  const double one = 1.0, zero = 0.0;
+  for (auto& ch : chunks) {
+    const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
+    launch_eri3c_rows(p, ch.first, ch.second, r0, raw.p, ld, false, s);
+    // B[r0:r0+nr, :] = raw (nr x naux) . L (naux x ldb); column-major view: B^T = L^T raw^T
+    DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)p.ldb, (int)nr, (int)p.naux,
+                            &one, p.d_L.as<double>(), (int)p.naux, raw.as<double>(), (int)ld, &zero,
+                            p.d_B.as<double>() + r0 * p.ldb, (int)p.ldb));
+  }
+  check_finite(p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
+  p.built = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics: dense tensors in dftax's order
+// ---------------------------------------------------------------------------
+
+__global__ void scatter_dense3_kernel(const double* __restrict__ raw, int64_t nrows, int64_t naux,
+                                      int64_t row_base, const int* __restrict__ rm,
+                                      const int* __restrict__ rn, const int8_t* __restrict__ kind,
+                                      const int* __restrict__ perm, int64_t nao,
+                                      double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nrows * naux) return;
+  const int64_t r = i / naux, col = i % naux;
+  const int64_t gr = r + row_base;
+  const int m = rm[gr], n = rn[gr];
+  const double v = raw[i];
+  const int P = perm[col];
+  out[((int64_t)m * nao + n) * naux + P] = v;
+  if (kind[gr] == 2) out[((int64_t)n * nao + m) * naux + P] = v;
+}
+
+__global__ void unpermute2_kernel(const double* __restrict__ in, int64_t n,
+                                  const int* __restrict__ perm, double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * n) return;
+  const int64_t r = i / n, c = i % n;
+  out[(int64_t)perm[r] * n + perm[c]] = in[i];
+}
+
+void eri3c_dense(Plan& p, double* out, cudaStream_t s) {
+  const int64_t nao = p.nao, naux = p.naux;
+  DFJK_CUDA(cudaMemsetAsync(out, 0, (size_t)nao * nao * naux * sizeof(double), s));
+  launch_pair_setup(p, s);
+  auto chunks = pair_chunks(p, naux, chunk_budget(p));
+  int64_t maxrows = 1;
+  for (auto& ch : chunks) maxrows = std::max(maxrows, rows_of(p, ch.first, ch.second));
+  DevBuf raw;
+  raw.alloc((size_t)maxrows * naux * sizeof(double));
+  for (auto& ch : chunks) {
+    const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
+    launch_eri3c_rows(p, ch.first, ch.second, r0, raw.p, naux, false, s);
+    const int64_t tot = nr * naux;
+    scatter_dense3_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
+        raw.as<double>(), nr, naux, r0, p.d_row_m.as<int>(), p.d_row_n.as<int>(),
+        p.d_row_w.as<int8_t>(), p.d_aux_perm.as<int>(), nao, out);
+    DFJK_CUDA(cudaGetLastError());
+  }
+  DFJK_CUDA(cudaStreamSynchronize(s));
+}
+
+void eri2c_dense(Plan& p, double* out, cudaStream_t s) {
+  const int64_t n = p.naux;
+  DevBuf v;
+  v.alloc((size_t)n * n * sizeof(double));
+  DFJK_CUDA(cudaMemsetAsync(v.p, 0, (size_t)n * n * sizeof(double), s));
+  launch_eri2c(p, v.as<double>(), n, s);
+  unpermute2_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(v.as<double>(), n,
+                                                                     p.d_aux_perm.as<int>(), out);
+  DFJK_CUDA(cudaGetLastError());
+  DFJK_CUDA(cudaStreamSynchronize(s));
+}
+
+void metric_pinv(Plan& p, double* out, cudaStream_t s) {
+  if (!p.built) fail(DFJK_ERR_STATE, "metric_pinv before dfjk_build");
+  Context& c = *p.ctx;
+  const int64_t n = p.naux;
+  DevBuf v;
+  v.alloc((size_t)n * n * sizeof(double));
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  const double one = 1.0, zero = 0.0;
+  // V+ = L L^T (column-major L: naux x ldb)
+  DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_T, (int)n, (int)n, (int)p.ldb, &one,
+                          p.d_L.as<double>(), (int)n, p.d_L.as<double>(), (int)n, &zero,
+                          v.as<double>(), (int)n));
+  unpermute2_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(v.as<double>(), n,
+                                                                     p.d_aux_perm.as<int>(), out);
+  DFJK_CUDA(cudaGetLastError());
+  DFJK_CUDA(cudaStreamSynchronize(s));
+}
+
+double energy(Plan& p, const double* P, int nspin, double hf, double* F, cudaStream_t s);
+
+}  // namespace dfjk
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+using namespace dfjk;
+
+template <class Fn>
+static dfjk_status guard(Context* c, Fn&& fn) {
+  try {
+    fn();
+    if (c) c->last_error.clear();
+    return DFJK_OK;
+  } catch (const Error& e) {
+    if (c) c->last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (c) c->last_error = "host allocation failed";
+    return DFJK_ERR_MEMORY;
+  } catch (const std::exception& e) {
+    if (c) c->last_error = e.what();
+    return DFJK_ERR_INVALID;
+  }
+}
+
+static cudaStream_t st(void* s) { return static_cast<cudaStream_t>(s); }
+
+extern "C" {
+
+void dfjk_default_options(dfjk_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->screen = 0.0;
+  o->metric_cutoff = 1e-7;
+  o->precision = DFJK_FP64;
+  o->chunk_bytes = 0;
+}
+
+dfjk_status dfjk_create(int device, dfjk_ctx** out) {
+  if (!out) return DFJK_ERR_INVALID;
+  *out = nullptr;
+  dfjk_ctx* h = new (std::nothrow) dfjk_ctx;
+  if (!h) return DFJK_ERR_MEMORY;
+  dfjk_status st_ = guard(nullptr, [&] {
+    int n = 0;
+    DFJK_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) fail(DFJK_ERR_INVALID, "device %d out of range (%d)", device, n);
+    DFJK_CUDA(cudaSetDevice(device));
+    h->c.device = device;
+    DFJK_CUBLAS(cublasCreate(&h->c.cublas));
+    DFJK_CUSOLVER(cusolverDnCreate(&h->c.cusolver));
+    std::vector<double> tbl, asym;
+    boys_table_host(tbl, asym);
+    upload(h->c.boys, tbl);
+    upload(h->c.boys_asym, asym);
+  });
+  if (st_ != DFJK_OK) {
+    delete h;
+    return st_;
+  }
+  *out = h;
+  return DFJK_OK;
+}
+
+dfjk_status dfjk_destroy(dfjk_ctx* h) {
+  if (!h) return DFJK_OK;
+  cudaSetDevice(h->c.device);
+  if (h->c.cublas) cublasDestroy(h->c.cublas);
+  if (h->c.cusolver) cusolverDnDestroy(h->c.cusolver);
+  delete h;
+  return DFJK_OK;
+}
+
+const char* dfjk_last_error(const dfjk_ctx* h) { return h ? h->c.last_error.c_str() : "null context"; }
+
+dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basis* aux,
+                             const dfjk_options* opts, dfjk_plan** out) {
+  if (!h || !out) return DFJK_ERR_INVALID;
+  *out = nullptr;
+  dfjk_plan* pl = new (std::nothrow) dfjk_plan;
+  if (!pl) return DFJK_ERR_MEMORY;
+  dfjk_status r = guard(&h->c, [&] {
+    DFJK_CUDA(cudaSetDevice(h->c.device));
+    pl->p.ctx = &h->c;
+    if (opts) pl->p.opts = *opts;
+    else dfjk_default_options(&pl->p.opts);
+    if (!(pl->p.opts.metric_cutoff >= 0.0) || !std::isfinite(pl->p.opts.screen))
+      fail(DFJK_ERR_INVALID, "invalid options");
+    if (pl->p.opts.precision != DFJK_FP64 && pl->p.opts.precision != DFJK_MIXED)
+      fail(DFJK_ERR_INVALID, "unknown precision %d", pl->p.opts.precision);
+    make_plan(pl->p, orb, aux);
+  });
+  if (r != DFJK_OK) {
+    delete pl;
+    return r;
+  }
+  *out = pl;
+  return DFJK_OK;
+}
+
+dfjk_status dfjk_plan_destroy(dfjk_plan* pl) {
+  if (!pl) return DFJK_OK;
+  cudaSetDevice(pl->p.ctx->device);
+  delete pl;
+  return DFJK_OK;
+}
+
+dfjk_status dfjk_plan_get_info(const dfjk_plan* pl, dfjk_plan_info* info) {
+  if (!pl || !info) return DFJK_ERR_INVALID;
+  const Plan& p = pl->p;
+  info->nao = p.nao;
+  info->naux = p.naux;
+  info->nao_cart = p.orb.ncart;
+  info->naux_cart = p.aux.ncart;
+  info->nshell = p.orb.n;
+  info->naux_shell = p.aux.n;
+  info->npair_shell = (int64_t)p.pair_s1.size();
+  info->nrows = p.nrows;
+  info->nfit = p.nfit;
+  info->b_bytes = (int64_t)p.d_B.bytes;
+  info->built = p.built;
+  info->precision = p.opts.precision;
+  return DFJK_OK;
+}
+
+dfjk_status dfjk_build(dfjk_plan* pl, void* stream) {
+  if (!pl) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
+    build(pl->p, st(stream));
+  });
+}
+
+dfjk_status dfjk_jk(dfjk_plan* pl, const double* C, const double* w, int64_t ncol, double* J,
+                    double* K, void* stream) {
+  if (!pl) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    if (!pl->p.built) fail(DFJK_ERR_STATE, "dfjk_jk before dfjk_build");
+    if (!C || ncol <= 0) fail(DFJK_ERR_INVALID, "C is null or ncol=%lld", (long long)ncol);
+    DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
+    jk_compute(pl->p, C, w, ncol, J, K, st(stream));
+  });
+}
+
+dfjk_status dfjk_jk_host(dfjk_plan* pl, const double* C, const double* w, int64_t ncol, double* J,
+                         double* K, void* stream) {
+  if (!pl) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    Plan& p = pl->p;
+    if (!p.built) fail(DFJK_ERR_STATE, "dfjk_jk_host before dfjk_build");
+    if (!C || ncol <= 0) fail(DFJK_ERR_INVALID, "C is null or ncol=%lld", (long long)ncol);
+    DFJK_CUDA(cudaSetDevice(p.ctx->device));
+    cudaStream_t s = st(stream);
+    const size_t nc = (size_t)p.nao * ncol * sizeof(double), nn = (size_t)p.nao * p.nao * sizeof(double);
+    DevBuf dC, dw, dJ, dK;
+    dC.alloc(nc);
+    DFJK_CUDA(cudaMemcpyAsync(dC.p, C, nc, cudaMemcpyHostToDevice, s));
+    if (w) {
+      dw.alloc(ncol * sizeof(double));
+      DFJK_CUDA(cudaMemcpyAsync(dw.p, w, ncol * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    if (J) dJ.alloc(nn);
+    if (K) dK.alloc(nn);
+    jk_compute(p, dC.as<double>(), w ? dw.as<double>() : nullptr, ncol, J ? dJ.as<double>() : nullptr,
+               K ? dK.as<double>() : nullptr, s);
+    if (J) DFJK_CUDA(cudaMemcpyAsync(J, dJ.p, nn, cudaMemcpyDeviceToHost, s));
+    if (K) DFJK_CUDA(cudaMemcpyAsync(K, dK.p, nn, cudaMemcpyDeviceToHost, s));
+    DFJK_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+dfjk_status dfjk_energy(dfjk_plan* pl, const double* P, int32_t nspin, double hf_coeff, double* e,
+                        double* F, void* stream) {
+  if (!pl) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    if (!pl->p.built) fail(DFJK_ERR_STATE, "dfjk_energy before dfjk_build");
+    if (!P || !e || (nspin != 1 && nspin != 2)) fail(DFJK_ERR_INVALID, "bad energy arguments");
+    if (!std::isfinite(hf_coeff)) fail(DFJK_ERR_INVALID, "non-finite hf_coeff");
+    DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
+    *e = energy(pl->p, P, nspin, hf_coeff, F, st(stream));
+  });
+}
+
+dfjk_status dfjk_eri3c_dense(dfjk_plan* pl, double* out, void* stream) {
+  if (!pl || !out) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
+    eri3c_dense(pl->p, out, st(stream));
+  });
+}
+
+dfjk_status dfjk_eri2c_dense(dfjk_plan* pl, double* out, void* stream) {
+  if (!pl || !out) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
+    eri2c_dense(pl->p, out, st(stream));
+  });
+}
+
+dfjk_status dfjk_metric_pinv(dfjk_plan* pl, double* out, void* stream) {
+  if (!pl || !out) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
+    metric_pinv(pl->p, out, st(stream));
+  });
+}
+
+dfjk_status dfjk_kept_pairs(const dfjk_plan* pl, int32_t* out) {
+  if (!pl || !out) return DFJK_ERR_INVALID;
+  const Plan& p = pl->p;
+  // dftax order: sorted by (ia, ib)
+  std::vector<std::pair<int, int>> v;
+  for (size_t i = 0; i < p.pair_orig_a.size(); ++i) v.push_back({p.pair_orig_a[i], p.pair_orig_b[i]});
+  std::sort(v.begin(), v.end());
+  for (size_t i = 0; i < v.size(); ++i) {
+    out[2 * i] = v[i].first;
+    out[2 * i + 1] = v[i].second;
+  }
+  return DFJK_OK;
+}
+
+dfjk_status dfjk_boys(dfjk_ctx* h, const double* t, int64_t n, int32_t nmax, double* out, void* stream) {
+  if (!h) return DFJK_ERR_INVALID;
+  return guard(&h->c, [&] {
+    if (!t || !out || n < 0 || nmax < 0 || nmax > 18) fail(DFJK_ERR_INVALID, "bad boys arguments");
+    DFJK_CUDA(cudaSetDevice(h->c.device));
+    launch_boys(h->c, t, n, nmax, out, st(stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,10 @@
+// Instantiations of the 3-center kernels of bra class (l1, l2) = (3, 0), see eri3c.cuh.
+#include "eri3c.cuh"
+
+namespace dfjk {
+
+bool launch_eri3c_30(int lc, dim3 grid, cudaStream_t s, const Eri3cArgs& a) {
+  return launch_lc<3, 0>(lc, grid, s, a);
+}
+
+}  // namespace dfjk

@@ -1,0 +1,200 @@
+// Internal declarations of the dfjk library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/dfjk.h"
+
+namespace dfjk {
+
+// Angular-momentum coverage of the compiled integral kernels.
+constexpr int kLmaxOrb = 3;   // orbital shells up to f
+constexpr int kLmaxAux = 4;   // auxiliary shells up to g
+
+// Boys table geometry (dftax/energy/boys.py:33-36).
+constexpr int kBoysOrder = 6;
+constexpr int kBoysNmax = 24;
+constexpr int kBoysNgrid = 401;
+constexpr double kBoysDt = 0.1;
+constexpr double kBoysTmax = 40.0;
+
+struct Error {
+  dfjk_status code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(dfjk_status code, const char* fmt, ...);
+
+#define DFJK_CUDA(call)                                                              \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      ::dfjk::fail(DFJK_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                   __FILE__, __LINE__);                                              \
+  } while (0)
+
+#define DFJK_CUBLAS(call)                                                            \
+  do {                                                                               \
+    cublasStatus_t s_ = (call);                                                      \
+    if (s_ != CUBLAS_STATUS_SUCCESS)                                                 \
+      ::dfjk::fail(DFJK_ERR_CUDA, "%s failed: cublas status %d (%s:%d)", #call, (int)s_, \
+                   __FILE__, __LINE__);                                              \
+  } while (0)
+
+#define DFJK_CUSOLVER(call)                                                          \
+  do {                                                                               \
+    cusolverStatus_t s_ = (call);                                                    \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                               \
+      ::dfjk::fail(DFJK_ERR_CUDA, "%s failed: cusolver status %d (%s:%d)", #call, (int)s_, \
+                   __FILE__, __LINE__);                                              \
+  } while (0)
+
+// Device buffer owned by a plan or context.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void alloc(size_t n);
+  void free();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+  ~DevBuf() { free(); }
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+template <class T>
+void upload(DevBuf& b, const std::vector<T>& v) {
+  b.alloc(v.size() * sizeof(T) + 16);
+  if (!v.empty()) DFJK_CUDA(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+// Shell table of one basis (host side and device mirror).
+struct Shells {
+  int n = 0;
+  std::vector<int> l, nprim, prim0, row0, out0, ncomp;
+  std::vector<double> cen;            // 3 per shell
+  std::vector<double> pexp, pcoef;    // per primitive
+  int ncart = 0, nout = 0, lmax = 0;
+  bool spherical = true;
+  // device
+  DevBuf d_l, d_nprim, d_prim0, d_cen, d_pexp, d_pcoef;
+  void reset() {
+    n = ncart = nout = lmax = 0;
+    spherical = true;
+    l.clear(); nprim.clear(); prim0.clear(); row0.clear(); out0.clear(); ncomp.clear();
+    cen.clear(); pexp.clear(); pcoef.clear();
+  }
+};
+
+// Transformation blocks, one per l: ncart(l) x nout(l), row-major, packed.
+struct Blocks {
+  std::vector<double> host;
+  int off[8] = {0};
+  DevBuf dev;
+  void reset() {
+    host.clear();
+    for (int& o : off) o = 0;
+  }
+};
+
+// Device-side views passed to kernels.
+struct ShellView {
+  const int* l;
+  const int* nprim;
+  const int* prim0;
+  const double* cen;
+  const double* pexp;
+  const double* pcoef;
+};
+
+struct Plan;
+
+struct Context {
+  int device = 0;
+  std::string last_error;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  DevBuf boys;   // kBoysNgrid x (kBoysNmax+1) doubles
+  DevBuf boys_asym;  // 0.5*Gamma(n+1/2), n = 0..kBoysNmax
+};
+
+struct ClassRange {   // a contiguous run of shell pairs of one (l1, l2) class
+  int l1, l2;
+  int64_t begin, count;      // into the pair arrays
+  int64_t pp_begin, pp_count;  // primitive pairs
+  int64_t esph_off;          // doubles into the Esph buffer
+};
+
+struct Plan {
+  Context* ctx = nullptr;
+  dfjk_options opts{};
+  Shells orb, aux;
+  Blocks c2s_orb, c2s_aux;
+  int nao = 0, naux = 0;
+  // kept shell pairs, ordered by class; s1 has the larger l
+  std::vector<int> pair_s1, pair_s2, pair_orig_a, pair_orig_b;
+  std::vector<int64_t> pair_row0, pair_pp0;
+  std::vector<int> pair_npp;
+  std::vector<ClassRange> classes;
+  int64_t nrows = 0, npp = 0, esph_doubles = 0;
+  // aux column layout: shells sorted by l, columns in that order
+  std::vector<int> aux_order;        // sorted position -> shell index
+  std::vector<int> aux_col0;         // per shell (original index) -> column
+  int aux_lbegin[8] = {0}, aux_lcount[8] = {0};
+  std::vector<int> aux_perm;         // column (permuted) -> dftax aux index
+  // device: pairs
+  DevBuf d_pair_s1, d_pair_s2, d_pair_row0, d_pair_pp0, d_pair_npp;
+  DevBuf d_pp_P, d_pp_g, d_pp_pref, d_esph;   // primitive-pair data
+  DevBuf d_pp_pair, d_pp_pa, d_pp_pb;         // primitive pair -> (pair, prim a, prim b)
+  DevBuf d_aux_sorted;   // sorted position -> aux shell index
+  DevBuf d_aux_perm;     // column -> dftax index
+  // rows -> (m, n) and weights; K lists (CSR over m)
+  DevBuf d_row_m, d_row_n, d_row_w, d_kptr, d_krow, d_kn;
+  // build products
+  int64_t nfit = 0, ldb = 0;
+  int built = 0;
+  DevBuf d_metric;   // naux x naux: V, then eigenvectors (column-major)
+  DevBuf d_w;        // eigenvalues
+  DevBuf d_L;        // naux x ldb factor (column-major, zero padded)
+  DevBuf d_B;        // nrows x ldb (row-major)
+  std::vector<double> w_host;
+  int64_t k0 = 0;    // first kept eigen-direction
+};
+
+// ---- kernels & launchers (md.cu) ----
+void boys_table_host(std::vector<double>& tbl, std::vector<double>& asym);
+void launch_boys(const Context& c, const double* t, int64_t n, int nmax, double* out, cudaStream_t s);
+void launch_pair_setup(Plan& p, cudaStream_t s);
+void launch_eri3c_rows(Plan& p, int64_t pair_begin, int64_t pair_end, int64_t row_base,
+                       void* out, int64_t ld, bool f32, cudaStream_t s);
+void launch_eri2c(Plan& p, double* out, int64_t ld, cudaStream_t s);
+void launch_schwarz(const Context& c, Shells& sh, const std::vector<int>& pa,
+                    const std::vector<int>& pb, std::vector<double>& qmax);
+
+// ---- contractions (jk.cu) ----
+void jk_compute(Plan& p, const double* C, const double* w, int64_t ncol, double* J, double* K,
+                cudaStream_t s);
+double j_energy_from_density(Plan& p, const double* Ptot, double* J, cudaStream_t s);
+
+void check_finite(const double* x, int64_t n, cudaStream_t s, const char* what);
+
+// solid harmonics (api.cu)
+void standard_block(int l, std::vector<double>& out);   // ncart(l) x (2l+1)
+
+inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+}  // namespace dfjk
+
+struct dfjk_ctx {
+  dfjk::Context c;
+};
+struct dfjk_plan {
+  dfjk::Plan p;
+};

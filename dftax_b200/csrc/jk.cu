@@ -1,0 +1,456 @@
+// J and K contractions over the fitted tensor B (float64 path).
+//
+// B is row-major [nrows][ldb]: one row per AO pair (m, n) of a kept shell
+// pair, one column per kept metric direction (B = (mn|P) L, L L^T = V+).
+//
+//   J: dvec[r] = w_r D[m, n]             (w_r = 2 off-diagonal pair, else 1)
+//      gamma   = B^T dvec                 (stream B once; CTA partials + reduce)
+//      J[m, n] = J[n, m] = B[r] . gamma   (stream B again; warp per row)
+//   K: X[m][x][i] = sum_{(r, n) in list(m)} B[r][x] C'[n][i]   (half transform)
+//      K = X X^T over the (x, i) index    (DSYRK), C' = C sqrt|w|
+// which are the P-gradients of dftax's DFCoulomb.energy (terms.py:592-613):
+// J = int3c (V+ gamma), K = einsum("mlP,PQ,nsQ,ls->mn") (hybrid.py:23-41).
+#include "internal.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace dfjk {
+
+// ---------------------------------------------------------------------------
+// J
+// ---------------------------------------------------------------------------
+
+__global__ void dvec_from_c_kernel(const double* __restrict__ C, const double* __restrict__ w,
+                                   int64_t ncol, const int* __restrict__ rm,
+                                   const int* __restrict__ rn, const int8_t* __restrict__ kind,
+                                   int64_t nrows, double* __restrict__ dvec) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nrows) return;
+  const int m = rm[warp], n = rn[warp];
+  const double* cm = C + (int64_t)m * ncol;
+  const double* cn = C + (int64_t)n * ncol;
+  double s = 0.0;
+  for (int64_t i = lane; i < ncol; i += 32) s += (w ? w[i] : 1.0) * cm[i] * cn[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) dvec[warp] = (kind[warp] == 2 ? 2.0 : 1.0) * s;
+}
+
+__global__ void dvec_from_density_kernel(const double* __restrict__ D, int64_t nao,
+                                         const int* __restrict__ rm, const int* __restrict__ rn,
+                                         const int8_t* __restrict__ kind, int64_t nrows,
+                                         double* __restrict__ dvec) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= nrows) return;
+  const int m = rm[r], n = rn[r];
+  // off-diagonal pairs stand for both (m, n) and (n, m)
+  const double v = kind[r] == 2 ? D[(int64_t)m * nao + n] + D[(int64_t)n * nao + m]
+                                : D[(int64_t)m * nao + n];
+  dvec[r] = v;
+}
+
+// gamma partials: CTA (bx, by) sums rows [r0, r1) for columns [by*2048, +2048)
+constexpr int kGtThreads = 256;
+constexpr int kGtCols = kGtThreads * 8;
+
+__global__ void __launch_bounds__(kGtThreads) gamma_partial_kernel(
+    const double* __restrict__ B, int64_t ldb, int64_t nrows, const double* __restrict__ dvec,
+    int64_t rows_per_cta, double* __restrict__ part) {
+  const int64_t r0 = blockIdx.x * rows_per_cta;
+  const int64_t r1 = min(nrows, r0 + rows_per_cta);
+  const int64_t c0 = (int64_t)blockIdx.y * kGtCols + 2 * threadIdx.x;
+  double2 acc[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) acc[j] = make_double2(0.0, 0.0);
+  for (int64_t r = r0; r < r1; ++r) {
+    const double d = __ldg(dvec + r);
+    const double* row = B + r * ldb;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t c = c0 + j * 2 * kGtThreads;
+      if (c < ldb) {
+        const double2 b = __ldcs(reinterpret_cast<const double2*>(row + c));
+        acc[j].x += d * b.x;
+        acc[j].y += d * b.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t c = c0 + j * 2 * kGtThreads;
+    if (c < ldb) *reinterpret_cast<double2*>(part + blockIdx.x * ldb + c) = acc[j];
+  }
+}
+
+__global__ void reduce_rows_kernel(const double* __restrict__ part, int64_t nparts, int64_t ldb,
+                                   double* __restrict__ out) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= ldb) return;
+  double s = 0.0;
+  for (int64_t p = 0; p < nparts; ++p) s += part[p * ldb + c];
+  out[c] = s;
+}
+
+// J rows: one warp per row, J[m, n] and J[n, m]
+__global__ void j_rows_kernel(const double* __restrict__ B, int64_t ldb, int64_t nrows,
+                              const double* __restrict__ gamma, const int* __restrict__ rm,
+                              const int* __restrict__ rn, const int8_t* __restrict__ kind,
+                              int64_t nao, double* __restrict__ J) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < nrows; r += nwarps) {
+    const double* row = B + r * ldb;
+    double s = 0.0;
+    for (int64_t c = 2 * lane; c < ldb; c += 64) {
+      const double2 b = __ldcs(reinterpret_cast<const double2*>(row + c));
+      const double2 g = __ldg(reinterpret_cast<const double2*>(gamma + c));
+      s += b.x * g.x + b.y * g.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      const int k = kind[r];
+      if (k == 0) continue;
+      const int m = rm[r], n = rn[r];
+      J[(int64_t)m * nao + n] = s;
+      J[(int64_t)n * nao + m] = s;
+    }
+  }
+}
+
+static int num_sms(int dev) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 148;
+}
+
+// gamma = B^T dvec into `gamma` (ldb doubles)
+static void gamma_from_dvec(Plan& p, const double* dvec, double* gamma, cudaStream_t s) {
+  const int sms = num_sms(p.ctx->device);
+  const int64_t ycols = (p.ldb + kGtCols - 1) / kGtCols;
+  int64_t xparts = std::max<int64_t>(1, (int64_t)sms * 4 / ycols);
+  xparts = std::min<int64_t>(xparts, std::max<int64_t>(1, p.nrows));
+  const int64_t rows_per = (p.nrows + xparts - 1) / xparts;
+  xparts = (p.nrows + rows_per - 1) / rows_per;
+  DevBuf part;
+  part.alloc((size_t)std::max<int64_t>(xparts, 1) * p.ldb * sizeof(double));
+  if (p.nrows > 0) {
+    gamma_partial_kernel<<<dim3((unsigned)xparts, (unsigned)ycols), kGtThreads, 0, s>>>(
+        p.d_B.as<double>(), p.ldb, p.nrows, dvec, rows_per, part.as<double>());
+    DFJK_CUDA(cudaGetLastError());
+    reduce_rows_kernel<<<(unsigned)((p.ldb + 255) / 256), 256, 0, s>>>(part.as<double>(), xparts,
+                                                                       p.ldb, gamma);
+    DFJK_CUDA(cudaGetLastError());
+  } else {
+    DFJK_CUDA(cudaMemsetAsync(gamma, 0, p.ldb * sizeof(double), s));
+  }
+}
+
+static void j_from_gamma(Plan& p, const double* gamma, double* J, cudaStream_t s) {
+  DFJK_CUDA(cudaMemsetAsync(J, 0, (size_t)p.nao * p.nao * sizeof(double), s));
+  if (p.nrows == 0) return;
+  const int sms = num_sms(p.ctx->device);
+  const int64_t warps = std::min<int64_t>(p.nrows, (int64_t)sms * 64);
+  j_rows_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
+      p.d_B.as<double>(), p.ldb, p.nrows, gamma, p.d_row_m.as<int>(), p.d_row_n.as<int>(),
+      p.d_row_w.as<int8_t>(), p.nao, J);
+  DFJK_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// K: half transform X[m][x][i] = sum_{(r, n) in list(m)} B[r][x0 + x] C'[n][i]
+// ---------------------------------------------------------------------------
+
+constexpr int kHtX = 64, kHtI = 64, kHtK = 16;
+
+__global__ void __launch_bounds__(256) half_transform_kernel(
+    const double* __restrict__ B, int64_t ldb, int64_t x0, int64_t xc, const double* __restrict__ Cp,
+    int64_t ncol, const int* __restrict__ kptr, const int* __restrict__ krow,
+    const int* __restrict__ kn, double* __restrict__ X) {
+  __shared__ double Bs[kHtK][kHtX];
+  __shared__ double Cs[kHtK][kHtI];
+  const int m = blockIdx.x;
+  const int64_t xt = (int64_t)blockIdx.y * kHtX;   // within the chunk
+  const int64_t it = (int64_t)blockIdx.z * kHtI;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  const int e0 = kptr[m], e1 = kptr[m + 1];
+  for (int e = e0; e < e1; e += kHtK) {
+    // stage kHtK list entries: rows of B (x tile) and rows of C' (i tile)
+    for (int q = threadIdx.x; q < kHtK * kHtX; q += 256) {
+      const int k = q / kHtX, x = q % kHtX;
+      double v = 0.0;
+      if (e + k < e1 && xt + x < xc) v = B[(int64_t)krow[e + k] * ldb + x0 + xt + x];
+      Bs[k][x] = v;
+    }
+    for (int q = threadIdx.x; q < kHtK * kHtI; q += 256) {
+      const int k = q / kHtI, i = q % kHtI;
+      double v = 0.0;
+      if (e + k < e1 && it + i < ncol) v = Cp[(int64_t)kn[e + k] * ncol + it + i];
+      Cs[k][i] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kHtK; ++k) {
+      double bx[4], ci[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) bx[a] = Bs[k][tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) ci[b] = Cs[k][ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += bx[a] * ci[b];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int64_t x = xt + tx + 16 * a;
+    if (x >= xc) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int64_t i = it + ty + 16 * b;
+      if (i < ncol) X[((int64_t)m * xc + x) * ncol + i] = acc[a][b];
+    }
+  }
+}
+
+__global__ void scale_cols_kernel(const double* __restrict__ C, const double* __restrict__ w,
+                                  int64_t nao, int64_t ncol, const int* __restrict__ sel,
+                                  int64_t nsel, double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nao * nsel) return;
+  const int64_t m = i / nsel, j = i % nsel;
+  const int col = sel[j];
+  const double f = w ? sqrt(fabs(w[col])) : 1.0;
+  out[i] = C[m * ncol + col] * f;
+}
+
+__global__ void symmetrize_kernel(double* __restrict__ K, int64_t n) {
+  // cuBLAS filled the column-major lower triangle = row-major upper (j >= i)
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * n) return;
+  const int64_t i = t / n, j = t % n;
+  if (j < i) K[t] = K[j * n + i];
+}
+
+// K (+)= sign * X X^T for the selected columns of C (scaled by sqrt|w|)
+static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol,
+                         const std::vector<int>& sel, double sign, bool first, double* K,
+                         cudaStream_t s) {
+  Context& c = *p.ctx;
+  const int64_t nao = p.nao, nsel = (int64_t)sel.size();
+  if (nsel == 0) return;
+  DevBuf dsel, Cp;
+  upload(dsel, sel);
+  Cp.alloc((size_t)nao * nsel * sizeof(double));
+  scale_cols_kernel<<<(unsigned)((nao * nsel + 255) / 256), 256, 0, s>>>(C, w, nao, ncol,
+                                                                         dsel.as<int>(), nsel,
+                                                                         Cp.as<double>());
+  DFJK_CUDA(cudaGetLastError());
+  // x chunking so that X (nao * xc * nsel doubles) stays within budget
+  const int64_t budget = (int64_t)6 << 30;
+  int64_t xc = budget / (nao * nsel * (int64_t)sizeof(double));
+  xc = std::max<int64_t>(kHtX, xc / kHtX * kHtX);
+  xc = std::min<int64_t>(xc, (p.nfit + kHtX - 1) / kHtX * kHtX);
+  DevBuf X;
+  X.alloc((size_t)nao * xc * nsel * sizeof(double));
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  bool beta0 = first;
+  for (int64_t x0 = 0; x0 < p.nfit; x0 += xc) {
+    const int64_t n = std::min(xc, p.nfit - x0);
+    dim3 grid((unsigned)nao, (unsigned)((n + kHtX - 1) / kHtX), (unsigned)((nsel + kHtI - 1) / kHtI));
+    half_transform_kernel<<<grid, 256, 0, s>>>(p.d_B.as<double>(), p.ldb, x0, n, Cp.as<double>(),
+                                               nsel, p.d_kptr.as<int>(), p.d_krow.as<int>(),
+                                               p.d_kn.as<int>(), X.as<double>());
+    DFJK_CUDA(cudaGetLastError());
+    // X row-major (nao x n*nsel) == column-major (n*nsel x nao): K = op(A) op(A)^T, op = T
+    const double alpha = sign, beta = beta0 ? 0.0 : 1.0;
+    DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)nao, (int)(n * nsel),
+                            &alpha, X.as<double>(), (int)(n * nsel), &beta, K, (int)nao));
+    beta0 = false;
+  }
+}
+
+static void k_compute(Plan& p, const double* C, const double* w, int64_t ncol, double* K,
+                      cudaStream_t s) {
+  std::vector<int> pos, neg;
+  if (w) {
+    std::vector<double> hw(ncol);
+    DFJK_CUDA(cudaMemcpyAsync(hw.data(), w, ncol * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DFJK_CUDA(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < ncol; ++i) {
+      if (!std::isfinite(hw[i])) fail(DFJK_ERR_NUMERIC, "non-finite weight");
+      if (hw[i] > 0) pos.push_back((int)i);
+      else if (hw[i] < 0) neg.push_back((int)i);
+    }
+  } else {
+    for (int64_t i = 0; i < ncol; ++i) pos.push_back((int)i);
+  }
+  if (pos.empty() && neg.empty()) {
+    DFJK_CUDA(cudaMemsetAsync(K, 0, (size_t)p.nao * p.nao * sizeof(double), s));
+    return;
+  }
+  k_accumulate(p, C, w, ncol, pos, 1.0, true, K, s);
+  k_accumulate(p, C, w, ncol, neg, -1.0, pos.empty(), K, s);
+  const int64_t n = p.nao;
+  symmetrize_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(K, n);
+  DFJK_CUDA(cudaGetLastError());
+}
+
+void jk_compute(Plan& p, const double* C, const double* w, int64_t ncol, double* J, double* K,
+                cudaStream_t s) {
+  if (J) {
+    DevBuf dvec, gamma;
+    dvec.alloc(std::max<int64_t>(p.nrows, 1) * sizeof(double));
+    gamma.alloc(p.ldb * sizeof(double));
+    if (p.nrows > 0) {
+      dvec_from_c_kernel<<<(unsigned)((p.nrows * 32 + 255) / 256), 256, 0, s>>>(
+          C, w, ncol, p.d_row_m.as<int>(), p.d_row_n.as<int>(), p.d_row_w.as<int8_t>(), p.nrows,
+          dvec.as<double>());
+      DFJK_CUDA(cudaGetLastError());
+    }
+    gamma_from_dvec(p, dvec.as<double>(), gamma.as<double>(), s);
+    j_from_gamma(p, gamma.as<double>(), J, s);
+  }
+  if (K) k_compute(p, C, w, ncol, K, s);
+}
+
+// ---------------------------------------------------------------------------
+// DFCoulomb.energy and its gradient
+// ---------------------------------------------------------------------------
+
+__global__ void add_kernel(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                           double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + b[i];
+}
+
+__global__ void dot_kernel(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                           double* __restrict__ out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += a[i] * b[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+__global__ void axpy_kernel(const double* __restrict__ x, double a, int64_t n, double* __restrict__ y) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] += a * x[i];
+}
+
+static double dot(const double* a, const double* b, int64_t n, cudaStream_t s) {
+  DevBuf r;
+  r.alloc(sizeof(double));
+  dot_kernel<<<1, 256, 0, s>>>(a, b, n, r.as<double>());
+  DFJK_CUDA(cudaGetLastError());
+  double h = 0;
+  DFJK_CUDA(cudaMemcpyAsync(&h, r.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+// K of a symmetric density Q (device, nao x nao): Q = V diag(l) V^T on the
+// device, K(Q) = sum_k l_k K(v_k v_k^T) over |l_k| > 1e-14 max|l|.
+static void k_of_density(Plan& p, const double* Q, double* K, cudaStream_t s) {
+  Context& c = *p.ctx;
+  const int64_t n = p.nao;
+  DevBuf V, wv, work, info;
+  V.alloc((size_t)n * n * sizeof(double));
+  wv.alloc(n * sizeof(double));
+  DFJK_CUDA(cudaMemcpyAsync(V.p, Q, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  DFJK_CUSOLVER(cusolverDnSetStream(c.cusolver, s));
+  int lwork = 0;
+  DFJK_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR,
+                                            CUBLAS_FILL_MODE_LOWER, (int)n, V.as<double>(), (int)n,
+                                            wv.as<double>(), &lwork));
+  work.alloc((size_t)std::max(lwork, 1) * sizeof(double));
+  info.alloc(sizeof(int));
+  DFJK_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                 (int)n, V.as<double>(), (int)n, wv.as<double>(), work.as<double>(),
+                                 lwork, info.as<int>()));
+  std::vector<double> hw(n);
+  int hinfo = 0;
+  DFJK_CUDA(cudaMemcpyAsync(hw.data(), wv.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  if (hinfo != 0) fail(DFJK_ERR_NUMERIC, "density eigensolver failed (info=%d)", hinfo);
+  double big = 0.0;
+  for (double v : hw) big = std::max(big, std::fabs(v));
+  // eigenvectors are the columns of the column-major V, i.e. rows of the
+  // row-major view: C[m][k] = V[k*n + m]; transpose into a row-major C
+  DevBuf Ct;
+  Ct.alloc((size_t)n * n * sizeof(double));
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  const double one = 1.0, zero = 0.0;
+  DFJK_CUBLAS(cublasDgeam(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)n, (int)n, &one, V.as<double>(),
+                          (int)n, &zero, V.as<double>(), (int)n, Ct.as<double>(), (int)n));
+  std::vector<double> wsel(n, 0.0);
+  for (int64_t k = 0; k < n; ++k)
+    if (std::fabs(hw[k]) > 1e-14 * big) wsel[k] = hw[k];
+  DevBuf dw;
+  upload(dw, wsel);
+  k_compute(p, Ct.as<double>(), dw.as<double>(), n, K, s);
+}
+
+double energy(Plan& p, const double* P, int nspin, double hf, double* F, cudaStream_t s) {
+  const int64_t n = p.nao, nn = n * n;
+  DevBuf Ptot, dvec, gamma, J;
+  const double* Pt = P;
+  if (nspin == 2) {
+    Ptot.alloc(nn * sizeof(double));
+    add_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(P, P + nn, nn, Ptot.as<double>());
+    DFJK_CUDA(cudaGetLastError());
+    Pt = Ptot.as<double>();
+  }
+  check_finite(P, nn * nspin, s, "the density");
+  dvec.alloc(std::max<int64_t>(p.nrows, 1) * sizeof(double));
+  gamma.alloc(p.ldb * sizeof(double));
+  if (p.nrows > 0) {
+    dvec_from_density_kernel<<<(unsigned)((p.nrows + 255) / 256), 256, 0, s>>>(
+        Pt, n, p.d_row_m.as<int>(), p.d_row_n.as<int>(), p.d_row_w.as<int8_t>(), p.nrows,
+        dvec.as<double>());
+    DFJK_CUDA(cudaGetLastError());
+  }
+  gamma_from_dvec(p, dvec.as<double>(), gamma.as<double>(), s);
+  double e = 0.5 * dot(gamma.as<double>(), gamma.as<double>(), p.ldb, s);
+  if (F) {
+    J.alloc(nn * sizeof(double));
+    j_from_gamma(p, gamma.as<double>(), J.as<double>(), s);
+    for (int sp = 0; sp < nspin; ++sp)
+      DFJK_CUDA(cudaMemcpyAsync(F + sp * nn, J.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  }
+  if (hf != 0.0) {
+    DevBuf K;
+    K.alloc(nn * sizeof(double));
+    for (int sp = 0; sp < nspin; ++sp) {
+      const double* Ps = P + sp * nn;
+      k_of_density(p, Ps, K.as<double>(), s);
+      const double tr = dot(Ps, K.as<double>(), nn, s);
+      // exchange quadratic (terms.py:500-509)
+      e += (nspin == 1 ? -0.25 : -0.5) * hf * tr;
+      if (F) {
+        const double a = (nspin == 1 ? -0.5 : -1.0) * hf;
+        axpy_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(K.as<double>(), a, nn, F + sp * nn);
+        DFJK_CUDA(cudaGetLastError());
+      }
+    }
+  }
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  return e;
+}
+
+}  // namespace dfjk

@@ -1,0 +1,147 @@
+/*
+ * dfjk.h — C ABI of the B200 density-fitting Coulomb/exchange library.
+ *
+ * The library replaces dftax's materialized density-fitting backend
+ * (dftax/ks/terms.py:576-613, class DFCoulomb) and the integral build that
+ * feeds it (dftax/ks/energy.py:406-433). All arguments are plain pointers and
+ * sizes; `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ * stream). Compute entry points take DEVICE pointers, as an XLA FFI handler
+ * receives them; the *_host variants take host pointers and copy in and out.
+ *
+ * Every call returns a dfjk_status; on failure dfjk_last_error(ctx) holds a
+ * one-line message. Invalid input, unsupported angular momentum, device
+ * memory refusal and non-finite values are reported, never trapped.
+ *
+ * A context or plan is not thread-safe: serialize calls that share one.
+ */
+#ifndef DFJK_H
+#define DFJK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dfjk_ctx dfjk_ctx;
+typedef struct dfjk_plan dfjk_plan;
+
+typedef enum {
+  DFJK_OK = 0,
+  DFJK_ERR_INVALID = 1,     /* bad argument: null pointer, size, basis layout   */
+  DFJK_ERR_UNSUPPORTED = 2, /* valid input beyond the kernels (l too high ...)  */
+  DFJK_ERR_CUDA = 3,        /* CUDA runtime, cuBLAS or cuSOLVER error           */
+  DFJK_ERR_MEMORY = 4,      /* device memory refused (budget or cudaMalloc)     */
+  DFJK_ERR_NUMERIC = 5,     /* non-finite value or failed eigensolver           */
+  DFJK_ERR_STATE = 6        /* call out of order, e.g. J/K before dfjk_build    */
+} dfjk_status;
+
+/* Precision of the build and contractions. */
+enum {
+  DFJK_FP64 = 0,  /* float64 integrals, B, J and K                               */
+  DFJK_MIXED = 1  /* float32 integrals and B; K on tensor cores in split bf16    */
+};
+
+/* Basis arrays in dftax's BasisData layout (dftax/energy/gto.py:132-156):
+ * one row per cartesian AO, host memory, row-major. */
+typedef struct {
+  int64_t ncart;              /* rows (cartesian AOs)                             */
+  int32_t max_prim;           /* padded primitive count per row                   */
+  int32_t nsph;               /* columns of cart2sph (ignored when it is NULL)    */
+  const double* centers;      /* [ncart][3], Bohr                                 */
+  const double* exponents;    /* [ncart][max_prim], zero padded                   */
+  const double* coefficients; /* [ncart][max_prim], zero padded                   */
+  const int32_t* angular;     /* [ncart][3] (lx, ly, lz)                          */
+  const double* cart2sph;     /* [ncart][nsph] block diagonal, or NULL            */
+} dfjk_basis;
+
+typedef struct {
+  double screen;        /* relative Schwarz shell-pair threshold; <= 0 keeps all
+                           (dftax df(screen=...), eri3c_bucketed.py:140-169)     */
+  double metric_cutoff; /* relative metric eigenvalue cutoff (terms.py:191)     */
+  int32_t precision;    /* DFJK_FP64 or DFJK_MIXED                               */
+  int32_t reserved;
+  int64_t chunk_bytes;  /* staging budget for raw 3-center rows (0 = default)   */
+} dfjk_options;
+
+typedef struct {
+  int64_t nao, naux;            /* spherical (or cartesian) AO / aux counts      */
+  int64_t nao_cart, naux_cart;
+  int64_t nshell, naux_shell;
+  int64_t npair_shell;          /* kept bra shell pairs                          */
+  int64_t nrows;                /* rows of B (AO pairs of the kept shell pairs)  */
+  int64_t nfit;                 /* columns of B (metric directions kept)         */
+  int64_t b_bytes;              /* device bytes held by B                        */
+  int32_t built;                /* 1 after a successful dfjk_build               */
+  int32_t precision;
+} dfjk_plan_info;
+
+/* Fill opts with dftax's defaults: screen off, cutoff 1e-7, FP64. */
+void dfjk_default_options(dfjk_options* opts);
+
+/* Context: device, library handles and the Boys table (dftax/energy/boys.py:81-123). */
+dfjk_status dfjk_create(int device, dfjk_ctx** ctx);
+dfjk_status dfjk_destroy(dfjk_ctx* ctx);
+const char* dfjk_last_error(const dfjk_ctx* ctx);
+
+/* Plan: shells, Schwarz-kept shell pairs, class buckets, device layout.
+ * Replaces plan_eri3c / plan_pairs / _shell_pair_keep
+ * (dftax/integrals/eri3c_bucketed.py:221-283, :448-483, :140-169) and the
+ * cart2sph checks (:186-218). Synchronizes the context's device. */
+dfjk_status dfjk_plan_create(dfjk_ctx* ctx, const dfjk_basis* orb, const dfjk_basis* aux,
+                             const dfjk_options* opts, dfjk_plan** plan);
+dfjk_status dfjk_plan_destroy(dfjk_plan* plan);
+dfjk_status dfjk_plan_get_info(const dfjk_plan* plan, dfjk_plan_info* info);
+
+/* Build: (P|Q) metric (eri3c_bucketed.py:746-779), its factor L with
+ * L L^T = V+ over eigenvalues above the cutoff (terms.py:155-192, :391-395),
+ * the 3-center (ij|P) (eri3c_bucketed.py:782-854) and B = (ij|P) L.
+ * Host-synchronizing (the kept-direction count sizes B). */
+dfjk_status dfjk_build(dfjk_plan* plan, void* stream);
+
+/* J and K of the density D = C diag(w) C^T (w == NULL: all ones), with
+ * C [nao][ncol] row-major on the device. J, K: [nao][nao] device outputs.
+ * J = sum_PQ (mn|P) V+_PQ (P|D), K = sum_PQ (ml|P) V+_PQ (ns|Q) D_ls
+ * (the gradients of DFCoulomb.energy, terms.py:592-613; K as in
+ * dftax/energy/hybrid.py:23-41 and terms.py:437-449). Either of J, K may be NULL. */
+dfjk_status dfjk_jk(dfjk_plan* plan, const double* C, const double* w, int64_t ncol,
+                    double* J, double* K, void* stream);
+
+/* Same with host buffers: copies C (and w) in, J and K out, then synchronizes. */
+dfjk_status dfjk_jk_host(dfjk_plan* plan, const double* C, const double* w, int64_t ncol,
+                         double* J, double* K, void* stream);
+
+/* DFCoulomb.energy (terms.py:592-613) and its P-gradient for the spin-stacked
+ * density P [nspin][nao][nao] (device): energy -> *e (host scalar) and, when
+ * F != NULL, dE/dP -> F [nspin][nao][nao] (device): J - a_x/2 K for nspin 1,
+ * J - a_x K_sigma for nspin 2 (terms.py:500-509). Any symmetric P is handled
+ * exactly (it is diagonalized on the device). Host-synchronizing. */
+dfjk_status dfjk_energy(dfjk_plan* plan, const double* P, int32_t nspin, double hf_coeff,
+                        double* e, double* F, void* stream);
+
+/* ---- parity / diagnostic entry points ---------------------------------- */
+
+/* Dense (nao, nao, naux) 3-center tensor in dftax's index order
+ * (eri3c_bucketed.py:782-854 output). Device output; requires a plan small
+ * enough for nao*nao*naux doubles. Does not need dfjk_build. */
+dfjk_status dfjk_eri3c_dense(dfjk_plan* plan, double* out, void* stream);
+
+/* (naux, naux) metric in dftax's order (eri3c_bucketed.py:746-779). */
+dfjk_status dfjk_eri2c_dense(dfjk_plan* plan, double* out, void* stream);
+
+/* V+ (naux, naux) in dftax's order after dfjk_build (terms.py:155-192). */
+dfjk_status dfjk_metric_pinv(dfjk_plan* plan, double* out, void* stream);
+
+/* Kept shell pairs as int32 [npair_shell][2] (ia <= ib, dftax shell order). Host output. */
+dfjk_status dfjk_kept_pairs(const dfjk_plan* plan, int32_t* out);
+
+/* Boys F_0..F_nmax at n points t (device): out [n][nmax+1]
+ * (dftax/energy/boys.py:130-176); nmax <= 18. */
+dfjk_status dfjk_boys(dfjk_ctx* ctx, const double* t, int64_t n, int32_t nmax, double* out,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFJK_H */

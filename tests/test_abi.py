@@ -1,0 +1,93 @@
+"""C ABI and host logic, no GPU needed: the library loads and exports every
+entry point include/dfjk.h declares; the synthetic workloads are what the
+configs describe."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from dftax_b200 import _lib, systems
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "dfjk.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return set(re.findall(r"\b(dfjk_[a-z0-9_]+)\s*\(", src))
+
+
+def test_exports_match_header():
+    assert header_functions() == set(_lib.EXPORTS)
+
+
+def test_library_loads_and_exports_every_symbol():
+    lib = _lib.load()
+    for name in header_functions():
+        assert getattr(lib, name) is not None
+    raw = ctypes.CDLL(_lib.LIB_PATH)
+    for name in header_functions():
+        ctypes.cast(getattr(raw, name), ctypes.c_void_p)
+
+
+def test_default_options():
+    lib = _lib.load()
+    o = _lib.Options()
+    lib.dfjk_default_options(ctypes.byref(o))
+    assert o.screen == 0.0 and o.metric_cutoff == 1e-7 and o.precision == _lib.DFJK_FP64
+
+
+def test_null_arguments_are_rejected_without_a_device():
+    lib = _lib.load()
+    assert lib.dfjk_create(0, None) == 1                     # INVALID
+    assert lib.dfjk_plan_get_info(None, None) == 1
+    assert lib.dfjk_build(None, None) == 1
+    assert lib.dfjk_jk(None, None, None, 0, None, None, None) == 1
+    assert lib.dfjk_last_error(None) == b"null context"
+
+
+def test_create_reports_missing_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    assert lib.dfjk_create(0, ctypes.byref(h)) != 0
+    assert not h.value
+
+
+def test_water_cluster_geometry():
+    sym, xyz = systems.water_cluster(32, seed=0)
+    o = xyz[0::3] / systems.ANGSTROM_TO_BOHR
+    d = np.linalg.norm(o[:, None] - o[None], axis=-1)
+    np.fill_diagonal(d, 99.0)
+    assert d.min() >= 2.6
+    side = (32 * systems.WATER_MASS / (systems.AVOGADRO * 1.0)) ** (1 / 3) * 1e8
+    assert abs(side - 9.86) < 0.01
+    # rigid monomers: O-H 0.9579 A
+    for k in range(32):
+        for h in (1, 2):
+            r = np.linalg.norm(xyz[3 * k + h] - xyz[3 * k]) / systems.ANGSTROM_TO_BOHR
+            assert abs(r - 0.957924) < 1e-5
+
+
+def test_alkane_geometry():
+    sym, xyz = systems.alkane(10, seed=0)
+    assert sym.count("C") == 10 and sym.count("H") == 22
+    a = xyz / systems.ANGSTROM_TO_BOHR
+    c = a[:10]
+    for i in range(9):
+        assert abs(np.linalg.norm(c[i + 1] - c[i]) - 1.54) < 1e-9
+    for h in a[10:]:
+        assert abs(np.min(np.linalg.norm(c - h, axis=1)) - 1.09) < 1e-9
+
+
+@pytest.mark.parametrize("name,nao,naux,nocc", [("water", 30, 141, 5), ("water8", 240, 1128, 40),
+                                                ("water32", 960, 4512, 160),
+                                                ("alkane10", 522, 2056, 41)])
+def test_workload_sizes(name, nao, naux, nocc):
+    _, _, orb, aux, no = systems.workload(name)
+    assert (orb.nao, aux.nao, no) == (nao, naux, nocc)

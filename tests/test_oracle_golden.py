@@ -1,0 +1,177 @@
+"""The CPU oracle against outputs of the reference itself (tests/golden/*.npz).
+
+Pins the oracle: Boys table and values, basis normalization and cart2sph,
+the bucketed 3-center and 2-center integrals, the metric pseudo-inverse, the
+DFCoulomb energy, J and K, and the Schwarz shell-pair screen. Tolerances:
+bitwise for the Boys table; 1e-13 absolute for integrals (both are float64
+evaluations of the same formulas in a different operation order); 1e-10
+relative for the energies and J/K (the tolerance the DF path is held to).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden_basis, load_golden, unpack_tril
+from oracle import boys as oboys
+from oracle import df as odf
+from oracle import md as omd
+
+
+def test_boys_table_is_bitwise_reference():
+    g = load_golden("boys")
+    assert np.array_equal(oboys.TABLE, g["table"])
+
+
+def test_boys_values_match_reference():
+    g = load_golden("boys")
+    vals = np.stack([oboys.boys(n, g["t"]) for n in range(19)])
+    np.testing.assert_allclose(vals, g["boys"], rtol=1e-14, atol=1e-16)
+    exact = np.stack([oboys.boys_exact(n, g["t"]) for n in range(19)])
+    np.testing.assert_allclose(exact, g["boys_exact"], rtol=1e-13, atol=1e-16)
+
+
+def test_boys_identities():
+    """F_n(0) = 1/(2n+1); dF_n/dt = -F_{n+1}; F_0 vs erf (test_boys_function.py:22-83)."""
+    from scipy.special import erf
+
+    for n in range(19):
+        assert abs(oboys.boys(n, np.array([0.0]))[0] - 1.0 / (2 * n + 1)) < 1e-14
+    t = np.linspace(0.05, 39.0, 200)
+    np.testing.assert_allclose(oboys.boys(0, t), np.sqrt(np.pi) / (2 * np.sqrt(t)) * erf(np.sqrt(t)),
+                               rtol=1e-11)
+    h = 1e-5
+    for n in range(0, 12):
+        d = (oboys.boys(n, t + h) - oboys.boys(n, t - h)) / (2 * h)
+        np.testing.assert_allclose(d, -oboys.boys(n + 1, t), rtol=1e-6, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["water", "ch2"])
+def test_basis_layout_matches_reference_loader(name):
+    from dftax_b200 import systems
+    from dftax_b200.basis import build_basis_data
+
+    g = load_golden(name)
+    sym = [str(s) for s in g["symbols"]]
+    for prefix, sets in (("orb", systems.ORBITAL_SETS), ("aux", systems.AUX_SETS)):
+        b = build_basis_data(sym, g["coords"], sets, spherical=True)
+        ref = golden_basis(g, prefix)
+        np.testing.assert_array_equal(b.angular, ref.angular)
+        np.testing.assert_array_equal(b.centers, ref.centers)
+        np.testing.assert_array_equal(b.exponents, ref.exponents)
+        np.testing.assert_allclose(b.coefficients, ref.coefficients, rtol=1e-15)
+        np.testing.assert_allclose(b.cart2sph, ref.cart2sph, atol=1e-14)
+
+
+def test_water_eri3c_matches_reference(water_golden):
+    g = water_golden
+    orb, aux = golden_basis(g, "orb"), golden_basis(g, "aux")
+    I3 = omd.eri3c(orb, aux)
+    nao = I3.shape[0]
+    ref = unpack_tril(g["int3c_tril"], nao)
+    assert np.abs(I3 - ref).max() < 1e-13
+    assert np.abs(I3 - I3.transpose(1, 0, 2)).max() < 1e-14
+
+
+def test_ch2_eri3c_high_l_matches_reference(ch2_golden):
+    """Orbital f and auxiliary g shells: every (la, lb | lc) class up to (ff|g)."""
+    g = ch2_golden
+    orb, aux = golden_basis(g, "orb"), golden_basis(g, "aux")
+    I3 = omd.eri3c(orb, aux)
+    v = I3[g["sample_m"], g["sample_n"], g["sample_P"]]
+    assert np.abs(v - g["sample_val"]).max() < 1e-13
+
+
+@pytest.mark.parametrize("name", ["water", "ch2"])
+def test_eri2c_and_metric_match_reference(name):
+    g = load_golden(name)
+    aux = golden_basis(g, "aux")
+    V = omd.eri2c(aux)
+    assert np.abs(V - g["int2c"]).max() < 1e-12
+    assert np.abs(V - V.T).max() < 1e-12
+    # metric pinv from the reference's own (P|Q)
+    vinv = odf.metric_pinv(g["int2c"])
+    ref = g["vinv"]
+    assert np.abs(vinv - ref).max() <= 1e-10 * np.abs(ref).max()
+    w = np.linalg.eigvalsh(g["int2c"])
+    assert int(np.sum(w > odf.CUTOFF * w[-1])) == int(g["n_kept"])
+
+
+def test_water_energy_j_k_match_reference(water_golden):
+    g = water_golden
+    nao = g["C"].shape[0]
+    I3 = unpack_tril(g["int3c_tril"], nao)
+    C = g["C"]
+    D = C @ C.T
+    P = 2.0 * D
+    # 1e-10 relative; the reference itself moves by ~3e-11 between einsum
+    # contraction orders (its K contracts through V+, condition ~1e8)
+    e = odf.df_energy(I3, g["vinv"], P[None], 0.25)
+    assert abs(e - g["e_total"]) <= 1e-10 * abs(g["e_total"])
+    assert abs(odf.df_energy(I3, g["vinv"], P[None], 0.0) - g["e_j"]) <= 1e-10 * abs(g["e_j"])
+    J, K = odf.df_jk(I3, g["vinv"], D)
+    assert np.linalg.norm(J - g["J"]) <= 1e-10 * np.linalg.norm(g["J"])
+    assert np.linalg.norm(K - g["K"]) <= 1e-10 * np.linalg.norm(g["K"])
+
+
+def test_k_from_metric_factor_equals_df_k(water_golden):
+    """K = sum_x (B_x C)(B_x C)^T with B = int3c L, L L^T = V+ (terms.py:437-449)."""
+    g = water_golden
+    nao = g["C"].shape[0]
+    I3 = unpack_tril(g["int3c_tril"], nao)
+    L = odf.metric_factor(g["int2c"])
+    B = np.einsum("mnP,Px->mnx", I3, L)
+    J, K = odf.jk_from_b(B, g["C"])
+    assert np.linalg.norm(J - g["J"]) <= 1e-10 * np.linalg.norm(g["J"])
+    assert np.linalg.norm(K - g["K"]) <= 1e-10 * np.linalg.norm(g["K"])
+
+
+# Metric noise floor. The CH2 metric has condition number ~1.9e8: the oracle's
+# (P|Q) differs from the reference's by 1.5e-13 (3e-16 relative), which moves
+# V+ by 7.5e-10 and J by 1.2e-10 relative. With the metric shared, the same
+# oracle matches J/K to 1.5e-11. A recomputed metric is therefore held to
+# NOISE_REL, the float64 floor of the reference's own formula.
+NOISE_REL = 5e-10
+
+
+def test_oracle_full_pipeline_matches_reference_energy(ch2_golden):
+    g = ch2_golden
+    orb, aux = golden_basis(g, "orb"), golden_basis(g, "aux")
+    I3 = omd.eri3c(orb, aux)
+    C = g["C"]
+    D = C @ C.T
+    # shared metric: the 1e-10 bar
+    e = odf.df_energy(I3, g["vinv"], (2.0 * D)[None], 0.25)
+    assert abs(e - g["e_total"]) <= 1e-10 * abs(g["e_total"])
+    J, K = odf.df_jk(I3, g["vinv"], D)
+    assert np.linalg.norm(J - g["J"]) <= 1e-10 * np.linalg.norm(g["J"])
+    assert np.linalg.norm(K - g["K"]) <= 1e-10 * np.linalg.norm(g["K"])
+    # recomputed metric: the noise floor
+    vinv = odf.metric_pinv(omd.eri2c(aux))
+    e = odf.df_energy(I3, vinv, (2.0 * D)[None], 0.25)
+    assert abs(e - g["e_total"]) <= NOISE_REL * abs(g["e_total"])
+    J, K = odf.df_jk(I3, vinv, D)
+    assert np.linalg.norm(J - g["J"]) <= NOISE_REL * np.linalg.norm(g["J"])
+    assert np.linalg.norm(K - g["K"]) <= NOISE_REL * np.linalg.norm(g["K"])
+
+
+def test_schwarz_keep_matches_reference(water_golden):
+    g = water_golden
+    orb = golden_basis(g, "orb")
+    keep = omd.shell_pair_keep(orb, float(g["screen_thresh"]))
+    ref = {(int(a), int(b)) for a, b in g["screen_keep"]}
+    assert keep == ref
+
+
+def test_occ_orbitals_recover_density(water_golden):
+    """_rik_occ_orbitals: C from P = 2 C C^T with S-orthonormal C (terms.py:369-388)."""
+    g = water_golden
+    rng = np.random.default_rng(3)
+    n = g["C"].shape[0]
+    A = rng.standard_normal((n, n))
+    S = A @ A.T / n + np.eye(n)
+    w, U = np.linalg.eigh(S)
+    Sih = (U / np.sqrt(w)) @ U.T
+    Cs = Sih @ np.linalg.qr(rng.standard_normal((n, 5)))[0]
+    P = 2.0 * Cs @ Cs.T
+    C = odf.occ_orbitals(P, S, 5)
+    np.testing.assert_allclose(2.0 * C @ C.T, P, atol=1e-12)
