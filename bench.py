@@ -1,0 +1,420 @@
+"""Benchmark of the DF J/K path: one line of JSON on rank 0.
+
+A step is one complete density-fitting J/K build for a (H2O)_32 cluster
+(960 spherical AOs, 4512 spherical auxiliary functions, 160 occupied
+orbitals, seeded geometry and C_occ): the (P|Q) metric and its factor, the
+3-center integrals, B = (ij|P) L, then J and K of D = C C^T. Inputs (basis
+arrays, C) are resident before the timed region; B (16.7 GB in float64) is
+larger than L2, so no explicit flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload water32] [--precision fp64|mixed]
+
+N > 1 runs under torchrun, one rank per GPU; each rank builds its own cluster
+(seeded by rank): the path has no exchange between molecules, so the ranks are
+independent replicas and ``value`` sums their builds ("scaling": "weak").
+``--impl reference`` times the CPU restatement of dftax's DF path (the oracle)
+on the host cores over a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "DF J/K builds/s"
+UNIT = "builds/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="water32")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on a bounded sample, scaled to the full workload
+# ---------------------------------------------------------------------------
+
+def cpu_build_seconds(workload: str, seed: int = 0, frac: float = 0.001):
+    """Estimated seconds of one full J/K build by the CPU oracle.
+
+    Sample: the oracle 3-center integrals for a seeded uniform sample of the
+    shell pairs (all auxiliary shells), scaled by the pair count; the oracle
+    (P|Q) for a sample of auxiliary shell pairs, scaled likewise; the full
+    metric eigendecomposition (LAPACK, all threads); and the dense BLAS work of
+    B = (ij|P) L, J and K on sampled rows / orbitals, scaled by their flops.
+    """
+    from dftax_b200 import systems
+    from oracle import md as omd
+
+    sym, xyz, orb, aux, nocc = systems.workload(workload, seed=seed)
+    rng = np.random.default_rng(1234)
+    sb = omd.shells(orb)
+    ns = len(sb)
+    ia, ib = np.triu_indices(ns)
+    npair = len(ia)
+    nsamp = max(64, int(frac * npair))
+    pick = rng.choice(npair, size=min(nsamp, npair), replace=False)
+    keep = {(int(ia[i]), int(ib[i])) for i in pick}
+    parts = {}
+    t0 = time.perf_counter()
+    rows = 0
+    for ra, rb, rc, v in omd.eri3c_blocks(orb, aux, keep):
+        rows += v.shape[0]
+    parts["eri3c"] = (time.perf_counter() - t0) * npair / len(keep)
+    # (P|Q): sample of the auxiliary basis (a sub-basis of whole shells)
+    sa = omd.shells(aux)
+    nsa = len(sa)
+    sub_n = max(40, int(nsa * 0.1))
+    sub = sorted(rng.choice(nsa, size=min(sub_n, nsa), replace=False).tolist())
+    rows_idx = np.concatenate([np.arange(sa[s][1], sa[s][1] + sa[s][2]) for s in sub])
+    from dftax_b200.basis import BasisData
+
+    subaux = BasisData(aux.centers[rows_idx], aux.exponents[rows_idx], aux.coefficients[rows_idx],
+                       aux.angular[rows_idx], None, aux.max_l)
+    t0 = time.perf_counter()
+    omd.eri2c(subaux)
+    parts["eri2c"] = (time.perf_counter() - t0) * (nsa * (nsa + 1) / 2) / (len(sub) * (len(sub) + 1) / 2)
+    naux, nao = aux.nao, orb.nao
+    ne = min(naux, 2048)
+    A = rng.standard_normal((ne, ne))
+    V = A @ A.T / ne + np.eye(ne)
+    t0 = time.perf_counter()
+    np.linalg.eigh(V)
+    parts["metric"] = (time.perf_counter() - t0) * (naux / ne) ** 3
+    nrows = nao * (nao + 1) // 2
+    sr = 4096
+    raw = rng.standard_normal((sr, naux))
+    L = rng.standard_normal((naux, naux))
+    t0 = time.perf_counter()
+    Bs = raw @ L
+    parts["bgemm"] = (time.perf_counter() - t0) * nrows / sr
+    d = rng.standard_normal(sr)
+    t0 = time.perf_counter()
+    g = Bs.T @ d
+    Bs @ g
+    parts["j"] = (time.perf_counter() - t0) * nrows / sr
+    C = rng.standard_normal((nao, nocc))
+    Bm = rng.standard_normal((nao, naux))
+    msamp = 8
+    t0 = time.perf_counter()
+    X = [Bm.T @ C for _ in range(msamp)]
+    parts["khalf"] = (time.perf_counter() - t0) * nao / msamp
+    kcols = 65536
+    Xs = rng.standard_normal((nao, kcols))
+    t0 = time.perf_counter()
+    Xs @ Xs.T
+    parts["ksyrk"] = (time.perf_counter() - t0) * (naux * nocc) / kcols * 0.5
+    del X
+    total = sum(parts.values())
+    sample = (f"oracle eri3c on {len(keep)} of {npair} shell pairs, (P|Q) on {len(sub)} of {nsa} "
+              f"aux shells, {ne}x{ne} eigh scaled by n^3, BLAS B/J/K on {sr} of {nrows} rows and "
+              f"{msamp} of {nao} half-transform rows; each part scaled to the full workload")
+    return total, parts, sample
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                c = [x.strip() for x in line.split(",")]
+                if len(c) >= 9 and c[0] == str(self.index):
+                    rows.append(c)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def fp64_gemm_peak(torch):
+    """Burst FP64 GEMM rate (cuBLAS DGEMM 8192^3, best of 5) in TFLOP/s."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def load_traffic(kernel: str, workload: str):
+    p = os.path.join(HERE, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    return d.get(f"{kernel}@{workload}")
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from dftax_b200 import Plan, _lib, systems
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device(f"cuda:{local_rank}"))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    sym, xyz, orb, aux, nocc = systems.workload(args.workload, seed=rank)
+    C = systems.random_occupied(orb.nao, nocc, seed=100 + rank)
+    plan = Plan(orb, aux, precision=args.precision)
+    Cd = torch.as_tensor(C, device="cuda")
+    J = torch.empty((orb.nao, orb.nao), dtype=torch.float64, device="cuda")
+    K = torch.empty_like(J)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.build(stream)
+        plan.jk(Cd, out=(J, K), stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    lib = _lib.load()
+    clocks = Clocks(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = lib.dfjk_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = (lib.dfjk_kernel_launches() - l0) // args.steps
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    phases = plan.phase_times()
+    info = plan.info()
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # per-iteration J/K with B resident (the SCF inner loop)
+    nit = 5
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(nit):
+        plan.jk(Cd, out=(J, K), stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    jk_ms = e0.elapsed_time(e1) / nit
+    jk_phases = plan.phase_times()
+
+    # end to end through the public host API: host basis arrays and C in,
+    # host J and K out, copies inside the timed region
+    Jh = np.empty((orb.nao, orb.nao))
+    Kh = np.empty_like(Jh)
+    h2d = sum(a.nbytes for b in (orb, aux) for a in (b.centers, b.exponents, b.coefficients,
+                                                      b.angular, b.cart2sph)) + C.nbytes
+    d2h = Jh.nbytes + Kh.nbytes
+    del plan
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        p2 = Plan(orb, aux, precision=args.precision)
+        p2.build(stream)
+        p2.jk_host(C, J=Jh, K=Kh, stream=stream)
+        p2.close()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * args.e2e_steps / (e2e_ms / 1e3)
+
+    # roofline of the dominant phase
+    hbm, bf16, src = measured_peaks()
+    fp64 = fp64_gemm_peak(torch) if rank == 0 else None
+    nrows, naux, nfit, nao = info["nrows"], info["naux"], info["nfit"], info["nao"]
+    ldb = (nfit + 7) // 8 * 8
+    units = {
+        "eri3c": ("hbm", 8.0 * nrows * naux / 1e9, "GB/s", hbm, "bytes of (ij|P) rows written"),
+        "bgemm": ("fp64", 2.0 * nrows * naux * ldb / 1e12, "TFLOP/s", fp64, "2 nrows naux nfit"),
+        "j": ("hbm", 2.0 * 8.0 * nrows * ldb / 1e9, "GB/s", hbm, "B streamed twice"),
+        "khalf": ("fp64", 2.0 * (2 * nrows - nao) * nfit * nocc / 1e12, "TFLOP/s", fp64,
+                  "2 sum_m |list(m)| nfit nocc"),
+        "ksyrk": ("fp64", 1.0 * nao * (nao + 1) * nfit * nocc / 1e12, "TFLOP/s", fp64,
+                  "nao (nao+1) nfit nocc"),
+    }
+    dom = max((k for k in units), key=lambda k: phases.get(k, 0.0))
+    bound, amount, unit, peak, what = units[dom]
+    achieved = amount / (phases[dom] / 1e3) if phases[dom] > 0 else 0.0
+    roof = {"kernel": dom, "bound": "hbm" if bound == "hbm" else "fp64",
+            "achieved": round(achieved, 3), "peak": round(peak, 3) if peak else None, "unit": unit,
+            "frac": round(achieved / peak, 4) if peak else None,
+            "peak_source": (f"{src} hbm_gbs" if bound == "hbm" else "in-bench cuBLAS DGEMM 8192^3 burst"),
+            "algorithmic": what, "ms_per_launch_group": round(phases[dom], 3),
+            "traffic": load_traffic(dom, args.workload)}
+
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+bf16x3", "data": "synthetic",
+        "config": {"workload": f"{args.workload} one DF J/K build from geometry (seeded)",
+                   "nao": nao, "naux": naux, "nocc": nocc, "nfit": nfit, "nrows": nrows,
+                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (B is %.1f GB)" % (8.0 * nrows * ldb / 1e9)},
+        "phases_ms": {k: round(v, 3) for k, v in phases.items() if k not in ("j", "khalf", "ksyrk")}
+        | {k: round(jk_phases[k], 3) for k in ("j", "khalf", "ksyrk")},
+        "jk_iteration": {"value": round(1e3 / jk_ms, 3), "unit": "J/K builds/s with B resident",
+                         "ms": round(jk_ms, 3)},
+        "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, parts, sample = cpu_build_seconds(args.workload)
+        line["cpu_baseline"] = {"value": round(1.0 / sec, 6), "unit": UNIT, "cores": cpu_cores(),
+                                "kind": "port", "sample": sample,
+                                "parts_s": {k: round(v, 3) for k, v in parts.items()}}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    sec, parts, sample = cpu_build_seconds(args.workload)
+    for _ in range(max(0, args.warmup - 1)):
+        pass  # the sample is re-timed per step below; warm-up is the first call above
+    vals = []
+    for _ in range(args.steps):
+        s, _p, _ = cpu_build_seconds(args.workload)
+        vals.append(s)
+    mean = float(np.mean(vals))
+    value = 1.0 / mean
+    line = {
+        "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{args.workload} one DF J/K build from geometry (seeded)",
+                   "precision": "fp64"},
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": cpu_cores(), "kind": "port",
+                         "sample": sample, "parts_s": {k: round(v, 3) for k, v in parts.items()}},
+        "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "dftax (JAX) is not installable here; the CPU restatement of its DF path is timed",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -149,6 +149,12 @@ class Plan:
     def naux(self) -> int:
         return self.info()["naux"]
 
+    def phase_times(self) -> dict:
+        """Milliseconds per phase of the last build and the last J/K call."""
+        arr = (ctypes.c_double * len(_lib.PHASES))()
+        check(self.lib.dfjk_phase_times(self.h, arr, len(_lib.PHASES)), self.ctx.h)
+        return dict(zip(_lib.PHASES, list(arr)))
+
     def build(self, stream=None):
         check(self.lib.dfjk_build(self.h, _stream_ptr(self.torch, stream)), self.ctx.h)
         return self

@@ -3,6 +3,7 @@
 #include "internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -29,6 +30,37 @@ void DevBuf::alloc(size_t n) {
     fail(DFJK_ERR_MEMORY, "cudaMalloc of %zu bytes failed: %s", n, cudaGetErrorString(e));
   }
   bytes = n;
+}
+
+static std::atomic<int64_t> g_launches{0};
+void count_launch(int64_t n) { g_launches += n; }
+
+void PhaseTimer::mark(int p, cudaStream_t s) {
+  if (used[p] == ev[p].size()) {
+    cudaEvent_t e;
+    DFJK_CUDA(cudaEventCreate(&e));
+    ev[p].push_back(e);
+  }
+  DFJK_CUDA(cudaEventRecord(ev[p][used[p]++], s));
+}
+
+double PhaseTimer::ms(int p) {
+  double tot = 0.0;
+  for (size_t i = 0; i + 1 < used[p]; i += 2) {
+    DFJK_CUDA(cudaEventSynchronize(ev[p][i + 1]));
+    float f = 0.f;
+    DFJK_CUDA(cudaEventElapsedTime(&f, ev[p][i], ev[p][i + 1]));
+    tot += f;
+  }
+  return tot;
+}
+
+void PhaseTimer::destroy() {
+  for (auto& v : ev) {
+    for (cudaEvent_t e : v) cudaEventDestroy(e);
+    v.clear();
+  }
+  for (auto& u : used) u = 0;
 }
 
 void DevBuf::free() {
@@ -417,13 +449,13 @@ __global__ void finite_check_kernel(const double* __restrict__ x, int64_t n, int
   if (i < n && !isfinite(x[i])) atomicExch(bad, 1);
 }
 
-void check_finite(const double* x, int64_t n, cudaStream_t s, const char* what) {
-  DevBuf flag;
-  flag.alloc(sizeof(int));
+void check_finite(Plan& p, const double* x, int64_t n, cudaStream_t s, const char* what) {
+  DevBuf& flag = p.ws_flag;
+  flag.ensure(sizeof(int));
   DFJK_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
   if (n > 0) {
     finite_check_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, n, flag.as<int>());
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
   }
   int h = 0;
   DFJK_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -438,19 +470,20 @@ static int64_t chunk_budget(const Plan& p) {
 void compute_metric_factor(Plan& p, cudaStream_t s) {
   Context& c = *p.ctx;
   const int64_t n = p.naux;
-  p.d_metric.alloc((size_t)n * n * sizeof(double));
+  p.d_metric.ensure((size_t)n * n * sizeof(double));
   DFJK_CUDA(cudaMemsetAsync(p.d_metric.p, 0, (size_t)n * n * sizeof(double), s));
   launch_eri2c(p, p.d_metric.as<double>(), n, s);
-  check_finite(p.d_metric.as<double>(), n * n, s, "the (P|Q) metric");
-  p.d_w.alloc(n * sizeof(double));
+  check_finite(p, p.d_metric.as<double>(), n * n, s, "the (P|Q) metric");
+  p.d_w.ensure(n * sizeof(double));
   DFJK_CUSOLVER(cusolverDnSetStream(c.cusolver, s));
   int lwork = 0;
   DFJK_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR,
                                             CUBLAS_FILL_MODE_LOWER, (int)n, p.d_metric.as<double>(),
                                             (int)n, p.d_w.as<double>(), &lwork));
-  DevBuf work, info;
-  work.alloc((size_t)std::max(lwork, 1) * sizeof(double));
-  info.alloc(sizeof(int));
+  DevBuf& work = p.ws_syevd;
+  DevBuf& info = p.ws_info;
+  work.ensure((size_t)std::max(lwork, 1) * sizeof(double));
+  info.ensure(sizeof(int));
   DFJK_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
                                  (int)n, p.d_metric.as<double>(), (int)n, p.d_w.as<double>(),
                                  work.as<double>(), lwork, info.as<int>()));
@@ -468,11 +501,11 @@ void compute_metric_factor(Plan& p, cudaStream_t s) {
   p.nfit = n - k0;
   if (p.nfit <= 0) fail(DFJK_ERR_NUMERIC, "metric has no eigenvalue above the cutoff");
   p.ldb = (p.nfit + 7) / 8 * 8;
-  p.d_L.alloc((size_t)n * p.ldb * sizeof(double));
+  p.d_L.ensure((size_t)n * p.ldb * sizeof(double));
   const int64_t tot = n * p.ldb;
   scale_factor_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
       p.d_metric.as<double>(), p.d_w.as<double>(), n, k0, p.nfit, p.ldb, p.d_L.as<double>());
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
 }
 
 // Pair chunks of at most `budget` bytes of raw rows (ld doubles each).
@@ -503,26 +536,35 @@ static int64_t rows_of(const Plan& p, int64_t b, int64_t e) {
 void build(Plan& p, cudaStream_t s) {
   Context& c = *p.ctx;
   p.built = 0;
+  for (int ph = kPhMetric; ph <= kPhBgemm; ++ph) p.timer.reset(ph);
+  p.timer.mark(kPhMetric, s);
   compute_metric_factor(p, s);
+  p.timer.mark(kPhMetric, s);
+  p.timer.mark(kPhPairs, s);
   launch_pair_setup(p, s);
-  p.d_B.alloc((size_t)std::max<int64_t>(p.nrows, 1) * p.ldb * sizeof(double));
+  p.timer.mark(kPhPairs, s);
+  p.d_B.ensure((size_t)std::max<int64_t>(p.nrows, 1) * p.ldb * sizeof(double));
   const int64_t ld = p.naux;
   auto chunks = pair_chunks(p, ld, chunk_budget(p));
   int64_t maxrows = 1;
   for (auto& ch : chunks) maxrows = std::max(maxrows, rows_of(p, ch.first, ch.second));
-  DevBuf raw;
-  raw.alloc((size_t)maxrows * ld * sizeof(double));
+  DevBuf& raw = p.ws_raw;
+  raw.ensure((size_t)maxrows * ld * sizeof(double));
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
   const double one = 1.0, zero = 0.0;
   for (auto& ch : chunks) {
     const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
+    p.timer.mark(kPhEri3c, s);
     launch_eri3c_rows(p, ch.first, ch.second, r0, raw.p, ld, false, s);
+    p.timer.mark(kPhEri3c, s);
     // B[r0:r0+nr, :] = raw (nr x naux) . L (naux x ldb); column-major view: B^T = L^T raw^T
+    p.timer.mark(kPhBgemm, s);
     DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)p.ldb, (int)nr, (int)p.naux,
                             &one, p.d_L.as<double>(), (int)p.naux, raw.as<double>(), (int)ld, &zero,
                             p.d_B.as<double>() + r0 * p.ldb, (int)p.ldb));
+    p.timer.mark(kPhBgemm, s);
   }
-  check_finite(p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
+  check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
   p.built = 1;
 }
 
@@ -570,7 +612,7 @@ void eri3c_dense(Plan& p, double* out, cudaStream_t s) {
     scatter_dense3_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
         raw.as<double>(), nr, naux, r0, p.d_row_m.as<int>(), p.d_row_n.as<int>(),
         p.d_row_w.as<int8_t>(), p.d_aux_perm.as<int>(), nao, out);
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
   }
   DFJK_CUDA(cudaStreamSynchronize(s));
 }
@@ -583,7 +625,7 @@ void eri2c_dense(Plan& p, double* out, cudaStream_t s) {
   launch_eri2c(p, v.as<double>(), n, s);
   unpermute2_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(v.as<double>(), n,
                                                                      p.d_aux_perm.as<int>(), out);
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
   DFJK_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -601,7 +643,7 @@ void metric_pinv(Plan& p, double* out, cudaStream_t s) {
                           v.as<double>(), (int)n));
   unpermute2_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(v.as<double>(), n,
                                                                      p.d_aux_perm.as<int>(), out);
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
   DFJK_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -814,6 +856,16 @@ dfjk_status dfjk_metric_pinv(dfjk_plan* pl, double* out, void* stream) {
     metric_pinv(pl->p, out, st(stream));
   });
 }
+
+dfjk_status dfjk_phase_times(dfjk_plan* pl, double* ms, int32_t n) {
+  if (!pl || !ms || n < 0) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    for (int i = 0; i < n && i < kPhCount; ++i) ms[i] = pl->p.timer.ms(i);
+    for (int i = kPhCount; i < n; ++i) ms[i] = 0.0;
+  });
+}
+
+int64_t dfjk_kernel_launches(void) { return g_launches.load(); }
 
 dfjk_status dfjk_kept_pairs(const dfjk_plan* pl, int32_t* out) {
   if (!pl || !out) return DFJK_ERR_INVALID;

@@ -14,6 +14,9 @@
 
 namespace dfjk {
 
+// Count of this library's kernel launches (host-side, all contexts).
+void count_launch(int64_t n = 1);
+
 // Angular-momentum coverage of the compiled integral kernels.
 constexpr int kLmaxOrb = 3;   // orbital shells up to f
 constexpr int kLmaxAux = 4;   // auxiliary shells up to g
@@ -56,12 +59,23 @@ struct Error {
                    __FILE__, __LINE__);                                              \
   } while (0)
 
+// After every kernel launch: surface launch errors and count the launch.
+#define DFJK_LAUNCHED()                 \
+  do {                                  \
+    DFJK_CUDA(cudaGetLastError());      \
+    ::dfjk::count_launch();             \
+  } while (0)
+
 // Device buffer owned by a plan or context.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   void alloc(size_t n);
   void free();
+  // grow-only: keep the allocation when it is already large enough
+  void ensure(size_t n) {
+    if (!p || bytes < n) alloc(n);
+  }
   template <class T> T* as() const { return static_cast<T*>(p); }
   ~DevBuf() { free(); }
   DevBuf() = default;
@@ -116,6 +130,20 @@ struct ShellView {
 
 struct Plan;
 
+// Phases timed with CUDA events on the call's stream (see dfjk_phase_times).
+enum Phase { kPhMetric = 0, kPhPairs, kPhEri3c, kPhBgemm, kPhJ, kPhKhalf, kPhKsyrk, kPhCount };
+
+struct PhaseTimer {
+  std::vector<cudaEvent_t> ev[kPhCount];   // begin/end pairs
+  size_t used[kPhCount] = {0};
+  void reset(int p) { used[p] = 0; }
+  void mark(int p, cudaStream_t s);        // records the next event of phase p
+  double ms(int p);                        // sum of elapsed over recorded pairs
+  void destroy();
+  ~PhaseTimer() { destroy(); }
+};
+
+
 struct Context {
   int device = 0;
   std::string last_error;
@@ -166,6 +194,9 @@ struct Plan {
   DevBuf d_B;        // nrows x ldb (row-major)
   std::vector<double> w_host;
   int64_t k0 = 0;    // first kept eigen-direction
+  PhaseTimer timer;
+  // persistent workspaces (grow-only), reused by every build and J/K call
+  DevBuf ws_raw, ws_syevd, ws_info, ws_flag, ws_dvec, ws_gamma, ws_part, ws_X, ws_Cp, ws_sel;
 };
 
 // ---- kernels & launchers (md.cu) ----
@@ -183,7 +214,7 @@ void jk_compute(Plan& p, const double* C, const double* w, int64_t ncol, double*
                 cudaStream_t s);
 double j_energy_from_density(Plan& p, const double* Ptot, double* J, cudaStream_t s);
 
-void check_finite(const double* x, int64_t n, cudaStream_t s, const char* what);
+void check_finite(Plan& p, const double* x, int64_t n, cudaStream_t s, const char* what);
 
 // solid harmonics (api.cu)
 void standard_block(int l, std::vector<double>& out);   // ncart(l) x (2l+1)

@@ -134,15 +134,15 @@ static void gamma_from_dvec(Plan& p, const double* dvec, double* gamma, cudaStre
   xparts = std::min<int64_t>(xparts, std::max<int64_t>(1, p.nrows));
   const int64_t rows_per = (p.nrows + xparts - 1) / xparts;
   xparts = (p.nrows + rows_per - 1) / rows_per;
-  DevBuf part;
-  part.alloc((size_t)std::max<int64_t>(xparts, 1) * p.ldb * sizeof(double));
+  DevBuf& part = p.ws_part;
+  part.ensure((size_t)std::max<int64_t>(xparts, 1) * p.ldb * sizeof(double));
   if (p.nrows > 0) {
     gamma_partial_kernel<<<dim3((unsigned)xparts, (unsigned)ycols), kGtThreads, 0, s>>>(
         p.d_B.as<double>(), p.ldb, p.nrows, dvec, rows_per, part.as<double>());
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
     reduce_rows_kernel<<<(unsigned)((p.ldb + 255) / 256), 256, 0, s>>>(part.as<double>(), xparts,
                                                                        p.ldb, gamma);
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
   } else {
     DFJK_CUDA(cudaMemsetAsync(gamma, 0, p.ldb * sizeof(double), s));
   }
@@ -156,7 +156,7 @@ static void j_from_gamma(Plan& p, const double* gamma, double* J, cudaStream_t s
   j_rows_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
       p.d_B.as<double>(), p.ldb, p.nrows, gamma, p.d_row_m.as<int>(), p.d_row_n.as<int>(),
       p.d_row_w.as<int8_t>(), p.nao, J);
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
 }
 
 // ---------------------------------------------------------------------------
@@ -248,33 +248,39 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
   Context& c = *p.ctx;
   const int64_t nao = p.nao, nsel = (int64_t)sel.size();
   if (nsel == 0) return;
-  DevBuf dsel, Cp;
-  upload(dsel, sel);
-  Cp.alloc((size_t)nao * nsel * sizeof(double));
+  DevBuf& dsel = p.ws_sel;
+  DevBuf& Cp = p.ws_Cp;
+  dsel.ensure(sel.size() * sizeof(int));
+  DFJK_CUDA(cudaMemcpyAsync(dsel.p, sel.data(), sel.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  Cp.ensure((size_t)nao * nsel * sizeof(double));
   scale_cols_kernel<<<(unsigned)((nao * nsel + 255) / 256), 256, 0, s>>>(C, w, nao, ncol,
                                                                          dsel.as<int>(), nsel,
                                                                          Cp.as<double>());
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
   // x chunking so that X (nao * xc * nsel doubles) stays within budget
   const int64_t budget = (int64_t)6 << 30;
   int64_t xc = budget / (nao * nsel * (int64_t)sizeof(double));
   xc = std::max<int64_t>(kHtX, xc / kHtX * kHtX);
   xc = std::min<int64_t>(xc, (p.nfit + kHtX - 1) / kHtX * kHtX);
-  DevBuf X;
-  X.alloc((size_t)nao * xc * nsel * sizeof(double));
+  DevBuf& X = p.ws_X;
+  X.ensure((size_t)nao * xc * nsel * sizeof(double));
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
   bool beta0 = first;
   for (int64_t x0 = 0; x0 < p.nfit; x0 += xc) {
     const int64_t n = std::min(xc, p.nfit - x0);
     dim3 grid((unsigned)nao, (unsigned)((n + kHtX - 1) / kHtX), (unsigned)((nsel + kHtI - 1) / kHtI));
+    p.timer.mark(kPhKhalf, s);
     half_transform_kernel<<<grid, 256, 0, s>>>(p.d_B.as<double>(), p.ldb, x0, n, Cp.as<double>(),
                                                nsel, p.d_kptr.as<int>(), p.d_krow.as<int>(),
                                                p.d_kn.as<int>(), X.as<double>());
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
+    p.timer.mark(kPhKhalf, s);
+    p.timer.mark(kPhKsyrk, s);
     // X row-major (nao x n*nsel) == column-major (n*nsel x nao): K = op(A) op(A)^T, op = T
     const double alpha = sign, beta = beta0 ? 0.0 : 1.0;
     DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)nao, (int)(n * nsel),
                             &alpha, X.as<double>(), (int)(n * nsel), &beta, K, (int)nao));
+    p.timer.mark(kPhKsyrk, s);
     beta0 = false;
   }
 }
@@ -302,23 +308,27 @@ static void k_compute(Plan& p, const double* C, const double* w, int64_t ncol, d
   k_accumulate(p, C, w, ncol, neg, -1.0, pos.empty(), K, s);
   const int64_t n = p.nao;
   symmetrize_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(K, n);
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
 }
 
 void jk_compute(Plan& p, const double* C, const double* w, int64_t ncol, double* J, double* K,
                 cudaStream_t s) {
+  for (int ph = kPhJ; ph <= kPhKsyrk; ++ph) p.timer.reset(ph);
   if (J) {
-    DevBuf dvec, gamma;
-    dvec.alloc(std::max<int64_t>(p.nrows, 1) * sizeof(double));
-    gamma.alloc(p.ldb * sizeof(double));
+    p.timer.mark(kPhJ, s);
+    DevBuf& dvec = p.ws_dvec;
+    DevBuf& gamma = p.ws_gamma;
+    dvec.ensure(std::max<int64_t>(p.nrows, 1) * sizeof(double));
+    gamma.ensure(p.ldb * sizeof(double));
     if (p.nrows > 0) {
       dvec_from_c_kernel<<<(unsigned)((p.nrows * 32 + 255) / 256), 256, 0, s>>>(
           C, w, ncol, p.d_row_m.as<int>(), p.d_row_n.as<int>(), p.d_row_w.as<int8_t>(), p.nrows,
           dvec.as<double>());
-      DFJK_CUDA(cudaGetLastError());
+      DFJK_LAUNCHED();
     }
     gamma_from_dvec(p, dvec.as<double>(), gamma.as<double>(), s);
     j_from_gamma(p, gamma.as<double>(), J, s);
+    p.timer.mark(kPhJ, s);
   }
   if (K) k_compute(p, C, w, ncol, K, s);
 }
@@ -356,7 +366,7 @@ static double dot(const double* a, const double* b, int64_t n, cudaStream_t s) {
   DevBuf r;
   r.alloc(sizeof(double));
   dot_kernel<<<1, 256, 0, s>>>(a, b, n, r.as<double>());
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
   double h = 0;
   DFJK_CUDA(cudaMemcpyAsync(&h, r.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   DFJK_CUDA(cudaStreamSynchronize(s));
@@ -413,17 +423,17 @@ double energy(Plan& p, const double* P, int nspin, double hf, double* F, cudaStr
   if (nspin == 2) {
     Ptot.alloc(nn * sizeof(double));
     add_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(P, P + nn, nn, Ptot.as<double>());
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
     Pt = Ptot.as<double>();
   }
-  check_finite(P, nn * nspin, s, "the density");
+  check_finite(p, P, nn * nspin, s, "the density");
   dvec.alloc(std::max<int64_t>(p.nrows, 1) * sizeof(double));
   gamma.alloc(p.ldb * sizeof(double));
   if (p.nrows > 0) {
     dvec_from_density_kernel<<<(unsigned)((p.nrows + 255) / 256), 256, 0, s>>>(
         Pt, n, p.d_row_m.as<int>(), p.d_row_n.as<int>(), p.d_row_w.as<int8_t>(), p.nrows,
         dvec.as<double>());
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
   }
   gamma_from_dvec(p, dvec.as<double>(), gamma.as<double>(), s);
   double e = 0.5 * dot(gamma.as<double>(), gamma.as<double>(), p.ldb, s);
@@ -445,7 +455,7 @@ double energy(Plan& p, const double* P, int nspin, double hf, double* F, cudaStr
       if (F) {
         const double a = (nspin == 1 ? -0.5 : -1.0) * hf;
         axpy_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(K.as<double>(), a, nn, F + sp * nn);
-        DFJK_CUDA(cudaGetLastError());
+        DFJK_LAUNCHED();
       }
     }
   }

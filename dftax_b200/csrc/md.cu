@@ -73,7 +73,7 @@ void launch_boys(const Context& c, const double* t, int64_t n, int nmax, double*
   int64_t blocks = (n + 255) / 256;
   boys_kernel<<<(unsigned)blocks, 256, 0, s>>>(t, n, nmax, c.boys.as<double>(),
                                                c.boys_asym.as<double>(), out);
-  DFJK_CUDA(cudaGetLastError());
+  DFJK_LAUNCHED();
 }
 
 // runtime versions of the packing helpers
@@ -400,7 +400,7 @@ void launch_pair_setup(Plan& p, cudaStream_t s) {
     DFJK_L1L2_CASES(X)
 #undef X
     if (!done) fail(DFJK_ERR_UNSUPPORTED, "pair class (%d,%d) not compiled", cr.l1, cr.l2);
-    DFJK_CUDA(cudaGetLastError());
+    DFJK_LAUNCHED();
   }
 }
 
@@ -441,7 +441,7 @@ void launch_eri3c_rows(Plan& p, int64_t pair_begin, int64_t pair_end, int64_t ro
         dim3 grid((unsigned)n, (unsigned)ychunks);
         const bool ok = launch_eri3c(cr.l1, cr.l2, lc, grid, s, a);
         if (!ok) fail(DFJK_ERR_UNSUPPORTED, "3-center class (%d,%d|%d) not compiled", cr.l1, cr.l2, lc);
-        DFJK_CUDA(cudaGetLastError());
+        DFJK_LAUNCHED();
       }
     }
   }
@@ -484,7 +484,7 @@ void launch_eri2c(Plan& p, double* out, int64_t ld, cudaStream_t s) {
       DFJK_LPLQ_CASES(X)
 #undef X
       if (!done) fail(DFJK_ERR_UNSUPPORTED, "aux class (%d,%d) not compiled", lp, lq);
-      DFJK_CUDA(cudaGetLastError());
+      DFJK_LAUNCHED();
     }
   }
 }
@@ -526,7 +526,7 @@ void launch_schwarz(const Context& c, Shells& sh, const std::vector<int>& pa,
       DFJK_L1L2_CASES(X)
 #undef X
       if (!done) fail(DFJK_ERR_UNSUPPORTED, "schwarz class (%d,%d) not compiled", l1, l2);
-      DFJK_CUDA(cudaGetLastError());
+      DFJK_LAUNCHED();
       std::vector<double> q(g.size());
       DFJK_CUDA(cudaMemcpy(q.data(), dq.p, g.size() * sizeof(double), cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < g.size(); ++i) qmax[g[i]] = q[i];

@@ -119,6 +119,29 @@ dfjk_status dfjk_jk_host(dfjk_plan* plan, const double* C, const double* w, int6
 dfjk_status dfjk_energy(dfjk_plan* plan, const double* P, int32_t nspin, double hf_coeff,
                         double* e, double* F, void* stream);
 
+/* ---- tracing ------------------------------------------------------------ */
+
+/* Phases timed with CUDA events on the stream of the last dfjk_build / dfjk_jk
+ * (dfjk_energy's J and K count as dfjk_jk). */
+enum {
+  DFJK_PHASE_METRIC = 0, /* (P|Q), eigensolver, factor L                      */
+  DFJK_PHASE_PAIRS = 1,  /* primitive-pair setup (E tables in spherical form) */
+  DFJK_PHASE_ERI3C = 2,  /* 3-center rows (all chunks)                        */
+  DFJK_PHASE_BGEMM = 3,  /* B = (ij|P) L (all chunks)                         */
+  DFJK_PHASE_J = 4,      /* gamma and J                                       */
+  DFJK_PHASE_KHALF = 5,  /* K half transform                                  */
+  DFJK_PHASE_KSYRK = 6,  /* K accumulation                                    */
+  DFJK_PHASE_COUNT = 7
+};
+
+/* Milliseconds per phase of the last build / J-K call: ms[0..n). Synchronizes
+ * on the recorded events. */
+dfjk_status dfjk_phase_times(dfjk_plan* plan, double* ms, int32_t n);
+
+/* Kernels this library has launched in this process (cuBLAS/cuSOLVER calls
+ * not included). */
+int64_t dfjk_kernel_launches(void);
+
 /* ---- parity / diagnostic entry points ---------------------------------- */
 
 /* Dense (nao, nao, naux) 3-center tensor in dftax's index order

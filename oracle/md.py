@@ -237,10 +237,23 @@ def _gather(basis, sh, idx):
 def eri3c(orb, aux, keep_pairs=None, chunk_elems=2_000_000):
     """Dense (nao, nao, naux) spherical 3-center tensor (both bra triangles)."""
     sb, sa = shells(orb), shells(aux)
-    sbs, nao = sph_starts(sb, orb.cart2sph)
-    sas, naux = sph_starts(sa, aux.cart2sph)
-    ang_o, ang_a = np.asarray(orb.angular), np.asarray(aux.angular)
+    _, nao = sph_starts(sb, orb.cart2sph)
+    _, naux = sph_starts(sa, aux.cart2sph)
     out = np.zeros((nao, nao, naux))
+    for ra, rb, rc, v in eri3c_blocks(orb, aux, keep_pairs, chunk_elems):
+        out[ra[:, :, None, None], rb[:, None, :, None], rc[:, None, None, :]] = v
+        out[rb[:, None, :, None], ra[:, :, None, None], rc[:, None, None, :]] = v
+    return out
+
+
+def eri3c_blocks(orb, aux, keep_pairs=None, chunk_elems=2_000_000):
+    """Yield (rows_a, rows_b, cols, values) per chunk of shell triples of one
+    class: values[t] is the spherical (na, nb, nc) block of triple t, written at
+    rows_a[t] x rows_b[t] x cols[t] of the dense tensor."""
+    sb, sa = shells(orb), shells(aux)
+    sbs, _ = sph_starts(sb, orb.cart2sph)
+    sas, _ = sph_starts(sa, aux.cart2sph)
+    ang_o, ang_a = np.asarray(orb.angular), np.asarray(aux.angular)
     for (la, lb, lc), (IA, IB, KC) in plan_eri3c(orb, aux, keep_pairs).items():
         anga = [tuple(ang_o[sb[IA[0]][1] + i]) for i in range(sb[IA[0]][2])]
         angb = [tuple(ang_o[sb[IB[0]][1] + i]) for i in range(sb[IB[0]][2])]
@@ -262,9 +275,7 @@ def eri3c(orb, aux, keep_pairs=None, chunk_elems=2_000_000):
             ra = sbs[ia][:, None] + np.arange(na)
             rb = sbs[ib][:, None] + np.arange(nb)
             rc = sas[kc][:, None] + np.arange(nc)
-            out[ra[:, :, None, None], rb[:, None, :, None], rc[:, None, None, :]] = v
-            out[rb[:, None, :, None], ra[:, :, None, None], rc[:, None, None, :]] = v
-    return out
+            yield ra, rb, rc, v
 
 
 # ---------------------------------------------------------------------------
