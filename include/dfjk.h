@@ -119,6 +119,19 @@ dfjk_status dfjk_jk_host(dfjk_plan* plan, const double* C, const double* w, int6
 dfjk_status dfjk_energy(dfjk_plan* plan, const double* P, int32_t nspin, double hf_coeff,
                         double* e, double* F, void* stream);
 
+/* J of D = C diag(w) C^T, as dfjk_jk computes it, without allocating any
+ * device memory: for callers that must not call cudaMalloc while they run
+ * (an XLA FFI handler inside a JAX program whose allocator already owns the
+ * GPU's memory; a serving loop that keeps cudaMalloc/cudaFree, which
+ * synchronize the device, off its hot path). No counterpart in the reference.
+ * Scratch is a fixed 16.8 MB array in the library's device memory, shared by
+ * all calls: plans whose B has more than 8192 columns are rejected
+ * (DFJK_ERR_UNSUPPORTED), and calls that overlap on the GPU race on it. The
+ * first call on a device looks up that array's address; make it before any
+ * stream capture. Float64 plans only. */
+dfjk_status dfjk_j_noalloc(dfjk_plan* plan, const double* C, const double* w, int64_t ncol,
+                           double* J, void* stream);
+
 /* ---- tracing ------------------------------------------------------------ */
 
 /* Phases timed with CUDA events on the stream of the last dfjk_build / dfjk_jk
