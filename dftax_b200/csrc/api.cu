@@ -422,6 +422,14 @@ static void make_plan(Plan& p, const dfjk_basis* orb, const dfjk_basis* aux) {
   p.d_esph.alloc(std::max<int64_t>(esph, 1) * sizeof(double));
   upload(p.d_aux_sorted, p.aux_order);
   upload(p.d_aux_perm, p.aux_perm);
+  {
+    std::vector<int> rowmap((size_t)p.nao * p.nao, -1);
+    for (int64_t r = 0; r < row; ++r) {
+      rowmap[(size_t)rm[r] * p.nao + rn[r]] = (int)r;
+      if (kind[r] == 2) rowmap[(size_t)rn[r] * p.nao + rm[r]] = (int)r;
+    }
+    upload(p.d_rowmap, rowmap);
+  }
   upload(p.d_row_m, rm);
   upload(p.d_row_n, rn);
   upload(p.d_row_w, kind);
@@ -565,6 +573,11 @@ void build(Plan& p, cudaStream_t s) {
     p.timer.mark(kPhBgemm, s);
   }
   check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
+  if (p.opts.precision == DFJK_MIXED) {
+    p.timer.mark(kPhBgemm, s);
+    build_ozaki_planes(p, s);
+    p.timer.mark(kPhBgemm, s);
+  }
   p.built = 1;
 }
 
@@ -769,7 +782,7 @@ dfjk_status dfjk_plan_get_info(const dfjk_plan* pl, dfjk_plan_info* info) {
   info->npair_shell = (int64_t)p.pair_s1.size();
   info->nrows = p.nrows;
   info->nfit = p.nfit;
-  info->b_bytes = (int64_t)p.d_B.bytes;
+  info->b_bytes = (int64_t)(p.d_B.bytes + p.d_oz_a.bytes);
   info->built = p.built;
   info->precision = p.opts.precision;
   return DFJK_OK;

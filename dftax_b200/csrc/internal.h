@@ -197,7 +197,18 @@ struct Plan {
   PhaseTimer timer;
   // persistent workspaces (grow-only), reused by every build and J/K call
   DevBuf ws_raw, ws_syevd, ws_info, ws_flag, ws_dvec, ws_gamma, ws_part, ws_X, ws_Cp, ws_sel;
+  // (m, n) -> row of B holding it, -1 when screened (both triangles)
+  DevBuf d_rowmap;
+  // mixed precision: int8 digit planes of the square B_x for the tensor-core half transform
+  DevBuf d_oz_a, d_oz_rowmax, d_oz_ea;
+  int64_t nao_p16 = 0;
+  DevBuf ws_oz_c, ws_oz_eb, ws_oz_err;
 };
+
+// ---- mixed-precision half transform (ozaki.cu) ----
+void build_ozaki_planes(Plan& p, cudaStream_t s);
+void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s);
+void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStream_t s);
 
 // ---- kernels & launchers (md.cu) ----
 void boys_table_host(std::vector<double>& tbl, std::vector<double>& asym);

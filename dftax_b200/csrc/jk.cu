@@ -270,10 +270,15 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
     const int64_t n = std::min(xc, p.nfit - x0);
     dim3 grid((unsigned)nao, (unsigned)((n + kHtX - 1) / kHtX), (unsigned)((nsel + kHtI - 1) / kHtI));
     p.timer.mark(kPhKhalf, s);
-    half_transform_kernel<<<grid, 256, 0, s>>>(p.d_B.as<double>(), p.ldb, x0, n, Cp.as<double>(),
-                                               nsel, p.d_kptr.as<int>(), p.d_krow.as<int>(),
-                                               p.d_kn.as<int>(), X.as<double>());
-    DFJK_LAUNCHED();
+    if (p.opts.precision == DFJK_MIXED) {
+      if (x0 == 0) ozaki_prepare_c(p, Cp.as<double>(), nsel, s);
+      ozaki_k1(p, nsel, x0, n, X.as<double>(), s);   // int8 tensor cores, exact accumulation
+    } else {
+      half_transform_kernel<<<grid, 256, 0, s>>>(p.d_B.as<double>(), p.ldb, x0, n, Cp.as<double>(),
+                                                 nsel, p.d_kptr.as<int>(), p.d_krow.as<int>(),
+                                                 p.d_kn.as<int>(), X.as<double>());
+      DFJK_LAUNCHED();
+    }
     p.timer.mark(kPhKhalf, s);
     p.timer.mark(kPhKsyrk, s);
     // X row-major (nao x n*nsel) == column-major (n*nsel x nao): K = op(A) op(A)^T, op = T

@@ -39,7 +39,9 @@ typedef enum {
 /* Precision of the build and contractions. */
 enum {
   DFJK_FP64 = 0,  /* float64 integrals, B, J and K                               */
-  DFJK_MIXED = 1  /* float32 integrals and B; K on tensor cores in split bf16    */
+  DFJK_MIXED = 1  /* float64 integrals, B and J; the K half transform on int8
+                     tensor cores (4 digits per value, exact int32 accumulation),
+                     extra 4*nfit*nao^2 bytes of device memory                  */
 };
 
 /* Basis arrays in dftax's BasisData layout (dftax/energy/gto.py:132-156):

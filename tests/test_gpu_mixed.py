@@ -1,0 +1,99 @@
+"""Mixed precision (DFJK_MIXED): the K half transform on int8 tensor cores.
+
+Tolerances, stated per quantity against the float64 form of the same plan
+(and against the reference's golden J/K where a fixture exists):
+  * J and the Coulomb energy: float64 in both forms, NOISE_REL as in the
+    float64 tests;
+  * K: 1e-7 relative (Frobenius). Four 7-bit digits per value keep 2^-27 of
+    each row's largest element; int32 accumulation adds no error, so what is
+    left is truncation (measured 3.5e-8 max-abs relative on water, 6.5e-9 on
+    (H2O)_32);
+  * total energy with a_x = 0.25: |dE| <= 1e-7 Ha (the target is 1 uHa;
+    measured 1e-9 Ha on water, 2.5e-10 Ha on (H2O)_32).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden_basis, load_golden
+
+pytestmark = pytest.mark.gpu
+
+NOISE_REL = 5e-10
+K_REL = 1e-7
+E_ABS = 1e-7
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _pair(orb, aux, **kw):
+    from dftax_b200 import Plan
+
+    return Plan(orb, aux, **kw).build(), Plan(orb, aux, precision="mixed", **kw).build()
+
+
+@pytest.mark.parametrize("name", ["water", "ch2"])
+def test_mixed_jk_and_energy_vs_reference(name):
+    from dftax_b200 import Plan
+
+    g = load_golden(name)
+    plan = Plan(golden_basis(g, "orb"), golden_basis(g, "aux"), precision="mixed").build()
+    assert plan.info()["precision"] == 1
+    J, K = plan.jk(g["C"])
+    J, K = J.cpu().numpy(), K.cpu().numpy()
+    assert rel(J, g["J"]) < NOISE_REL
+    assert rel(K, g["K"]) < K_REL
+    assert np.array_equal(K, K.T)
+    P = 2.0 * g["C"] @ g["C"].T
+    e, F = plan.energy(P, 0.25)
+    assert abs(e - g["e_total"]) < E_ABS
+    assert rel(F[0].cpu().numpy(), 2.0 * g["J"] - 0.25 * g["K"]) < K_REL
+
+
+@pytest.mark.parametrize("name,ncol", [("water8", None), ("water8", 100), ("alkane2", None)])
+def test_mixed_vs_fp64(name, ncol):
+    """Several 128-row and 80-column tiles (nao 240; 100 columns), f shells."""
+    from dftax_b200 import systems
+
+    sym, xyz, orb, aux, nocc = systems.workload(name, seed=3)
+    p64, pmx = _pair(orb, aux)
+    nao = p64.nao
+    C = systems.random_occupied(nao, ncol or nocc, seed=7)
+    J64, K64 = (x.cpu().numpy() for x in p64.jk(C))
+    Jm, Km = (x.cpu().numpy() for x in pmx.jk(C))
+    assert rel(Jm, J64) < 1e-14
+    assert rel(Km, K64) < K_REL
+    P = 2.0 * C @ C.T
+    e64, _ = p64.energy(P, 0.25, want_grad=False)
+    em, _ = pmx.energy(P, 0.25, want_grad=False)
+    assert abs(em - e64) < E_ABS
+
+
+def test_mixed_signed_weights_and_screening():
+    """Negative weights (the -sign DSYRK pass) and screened pairs (zero rows)."""
+    from dftax_b200 import systems
+
+    sym, xyz, orb, aux, nocc = systems.workload("water8", seed=1)
+    p64, pmx = _pair(orb, aux, screen=1e-8)
+    assert p64.info()["npair_shell"] < p64.info()["nshell"] * (p64.info()["nshell"] + 1) // 2
+    C = systems.random_occupied(p64.nao, 12, seed=2)
+    w = np.linspace(-1.0, 2.0, 12)
+    _, K64 = p64.jk(C, w)
+    _, Km = pmx.jk(C, w)
+    assert rel(Km.cpu().numpy(), K64.cpu().numpy()) < K_REL
+
+
+def test_mixed_is_deterministic():
+    """Integer accumulation: repeated calls give bit-identical K."""
+    from dftax_b200 import systems
+
+    sym, xyz, orb, aux, nocc = systems.workload("water3", seed=0)
+    from dftax_b200 import Plan
+
+    plan = Plan(orb, aux, precision="mixed").build()
+    C = systems.random_occupied(plan.nao, nocc, seed=1)
+    _, K1 = plan.jk(C)
+    _, K2 = plan.jk(C)
+    assert np.array_equal(K1.cpu().numpy(), K2.cpu().numpy())
