@@ -28,7 +28,7 @@ EXPORTS = (
     "dfjk_kept_pairs", "dfjk_boys", "dfjk_phase_times", "dfjk_kernel_launches",
     "dfjk_j_noalloc",
 )
-PHASES = ("metric", "pairs", "eri3c", "bgemm", "j", "khalf", "ksyrk")
+PHASES = ("metric", "pairs", "eri3c", "bgemm", "j", "khalf", "ksyrk", "kplanes")
 
 
 class LibraryNotLoaded(RuntimeError):

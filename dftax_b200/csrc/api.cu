@@ -422,14 +422,6 @@ static void make_plan(Plan& p, const dfjk_basis* orb, const dfjk_basis* aux) {
   p.d_esph.alloc(std::max<int64_t>(esph, 1) * sizeof(double));
   upload(p.d_aux_sorted, p.aux_order);
   upload(p.d_aux_perm, p.aux_perm);
-  {
-    std::vector<int> rowmap((size_t)p.nao * p.nao, -1);
-    for (int64_t r = 0; r < row; ++r) {
-      rowmap[(size_t)rm[r] * p.nao + rn[r]] = (int)r;
-      if (kind[r] == 2) rowmap[(size_t)rn[r] * p.nao + rm[r]] = (int)r;
-    }
-    upload(p.d_rowmap, rowmap);
-  }
   upload(p.d_row_m, rm);
   upload(p.d_row_n, rn);
   upload(p.d_row_w, kind);
@@ -545,6 +537,7 @@ void build(Plan& p, cudaStream_t s) {
   Context& c = *p.ctx;
   p.built = 0;
   for (int ph = kPhMetric; ph <= kPhBgemm; ++ph) p.timer.reset(ph);
+  p.timer.reset(kPhKplanes);
   p.timer.mark(kPhMetric, s);
   compute_metric_factor(p, s);
   p.timer.mark(kPhMetric, s);
@@ -560,23 +553,30 @@ void build(Plan& p, cudaStream_t s) {
   raw.ensure((size_t)maxrows * ld * sizeof(double));
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
   const double one = 1.0, zero = 0.0;
+  const bool mixed = p.opts.precision == DFJK_MIXED;
+  if (mixed) ozaki_prepare_l(p, s);
   for (auto& ch : chunks) {
     const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
     p.timer.mark(kPhEri3c, s);
     launch_eri3c_rows(p, ch.first, ch.second, r0, raw.p, ld, false, s);
     p.timer.mark(kPhEri3c, s);
-    // B[r0:r0+nr, :] = raw (nr x naux) . L (naux x ldb); column-major view: B^T = L^T raw^T
+    // B[r0:r0+nr, :] = raw (nr x naux) . L (naux x ldb)
     p.timer.mark(kPhBgemm, s);
-    DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)p.ldb, (int)nr, (int)p.naux,
-                            &one, p.d_L.as<double>(), (int)p.naux, raw.as<double>(), (int)ld, &zero,
-                            p.d_B.as<double>() + r0 * p.ldb, (int)p.ldb));
+    if (mixed) {
+      ozaki_bgemm(p, raw.as<double>(), nr, p.d_B.as<double>() + r0 * p.ldb, s);
+    } else {
+      // column-major view: B^T = L^T raw^T
+      DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)p.ldb, (int)nr, (int)p.naux,
+                              &one, p.d_L.as<double>(), (int)p.naux, raw.as<double>(), (int)ld,
+                              &zero, p.d_B.as<double>() + r0 * p.ldb, (int)p.ldb));
+    }
     p.timer.mark(kPhBgemm, s);
   }
   check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
-  if (p.opts.precision == DFJK_MIXED) {
-    p.timer.mark(kPhBgemm, s);
+  if (mixed) {
+    p.timer.mark(kPhKplanes, s);
     build_ozaki_planes(p, s);
-    p.timer.mark(kPhBgemm, s);
+    p.timer.mark(kPhKplanes, s);
   }
   p.built = 1;
 }

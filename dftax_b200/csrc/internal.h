@@ -131,7 +131,9 @@ struct ShellView {
 struct Plan;
 
 // Phases timed with CUDA events on the call's stream (see dfjk_phase_times).
-enum Phase { kPhMetric = 0, kPhPairs, kPhEri3c, kPhBgemm, kPhJ, kPhKhalf, kPhKsyrk, kPhCount };
+enum Phase {
+  kPhMetric = 0, kPhPairs, kPhEri3c, kPhBgemm, kPhJ, kPhKhalf, kPhKsyrk, kPhKplanes, kPhCount
+};
 
 struct PhaseTimer {
   std::vector<cudaEvent_t> ev[kPhCount];   // begin/end pairs
@@ -197,15 +199,17 @@ struct Plan {
   PhaseTimer timer;
   // persistent workspaces (grow-only), reused by every build and J/K call
   DevBuf ws_raw, ws_syevd, ws_info, ws_flag, ws_dvec, ws_gamma, ws_part, ws_X, ws_Cp, ws_sel;
-  // (m, n) -> row of B holding it, -1 when screened (both triangles)
-  DevBuf d_rowmap;
   // mixed precision: int8 digit planes of the square B_x for the tensor-core half transform
-  DevBuf d_oz_a, d_oz_rowmax, d_oz_ea;
-  int64_t nao_p16 = 0;
+  DevBuf d_oz_a, d_oz_ea;
+  int64_t nao_p16 = 0, naux_p16 = 0;
   DevBuf ws_oz_c, ws_oz_eb, ws_oz_err;
+  // mixed precision: digit planes of L^T (per build) and of one raw 3-center chunk
+  DevBuf ws_oz_l, ws_oz_el, ws_oz_raw, ws_oz_er;
 };
 
-// ---- mixed-precision half transform (ozaki.cu) ----
+// ---- mixed precision on the int8 tensor cores (ozaki.cu) ----
+void ozaki_prepare_l(Plan& p, cudaStream_t s);
+void ozaki_bgemm(Plan& p, const double* raw, int64_t nr, double* Bout, cudaStream_t s);
 void build_ozaki_planes(Plan& p, cudaStream_t s);
 void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s);
 void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStream_t s);

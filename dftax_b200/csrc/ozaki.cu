@@ -1,18 +1,27 @@
-// Mixed-precision K half transform (precision = DFJK_MIXED) on the int8
-// tensor cores with exact accumulation (ozaki_gemm.cu).
+// Mixed precision (precision = DFJK_MIXED): the two large products of the DF
+// path on the int8 tensor cores with exact accumulation (ozaki_gemm.cu):
+//   B[r][x] = sum_P (ij|P)[r][P] L[P][x]      (build, per raw row chunk)
+//   X[m][x][i] = sum_n B_x[m][n] C'[n][i]     (K half transform, per call)
+// Both operands of each product are split into signed 7-bit digits under a
+// per-row exponent; outputs are float64, and J, the metric, its factor L and
+// the K accumulation X X^T stay float64.
 //
-// Accuracy findings behind this design (device runs on water clusters):
+// Accuracy findings behind the digit counts (device runs on water clusters,
+// against the float64 path of the same plan):
 //   * storing the 3-center tensor or B in float32 moves E_J by 1.3 uHa already
-//     for (H2O)_4 (oracle simulation), so J and B stay float64;
+//     for (H2O)_4 (oracle simulation);
 //   * split-bf16 products accumulated in fp32 on the tensor cores bias K
 //     toward zero (relative -3e-6 with one 64-deep k tile per partial, -2.7e-4
-//     with long partials; E off by 76 uHa .. 5.9 mHa for (H2O)_32), so fp32
-//     accumulation cannot hold 1 uHa at these sizes;
+//     with long partials; E off by 76 uHa .. 5.9 mHa for (H2O)_32);
 //   * int8 digits with int32 accumulation are exact: what is left is the
-//     digit truncation (2^-27 of each row's largest value).
-// The half transform X[x][m][i] = sum_n B_x[m][n] C[n][i] therefore runs on
-// int8 digit planes of the square B_x (built once per geometry) and of C
-// (per call), and the float64 DSYRK of the float64 path finishes K.
+//     digit truncation, 2^(1-7D) of each row's largest value for D digits;
+//   * the half transform B_x C is well conditioned: 4 digits give K within
+//     6.5e-9 relative and E within 2.5e-10 Ha for (H2O)_32;
+//   * the build product (ij|P) L is not: the columns of L for small metric
+//     eigenvalues cancel the smooth part of each (ij|P) row, which amplifies
+//     the truncation by up to the metric's condition number. With 4 digits,
+//     E moved by 1.5e-5 Ha for (H2O)_8 and 1.0e-4 Ha for (H2O)_32, so the
+//     build uses 6 digits (2^-41), 2^14 times finer.
 #include "ozaki.h"
 
 #include <algorithm>
@@ -27,80 +36,146 @@ __device__ __forceinline__ int row_exponent(double vmax) {
   return vmax > 0.0 ? ilogb(vmax) + 2 : 0;
 }
 
-// four signed 7-bit digits: t = v 2^-e = sum_s d_s 2^(-7(s+1)) + O(2^-29)
-__device__ __forceinline__ void digits4(double v, int e, int8_t (&d)[4]) {
+// ND signed 7-bit digits: v 2^-e = sum_s d_s 2^(-7(s+1)) + r, |r| <= 2^(-7ND-1).
+// Every step is exact in float64: scaling by 128, rounding to an integer
+// (|d_s| <= 64) and subtracting it (|t - d_s| <= 1/2).
+template <int ND>
+__device__ __forceinline__ void digits(double v, int e, int8_t* d) {
   double t = ldexp(v, -e);
-  const double sc[4] = {0x1p7, 0x1p14, 0x1p21, 0x1p28};
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    const double q = rint(t * sc[s]);
+  for (int s = 0; s < ND; ++s) {
+    t *= 128.0;
+    const double q = rint(t);
     d[s] = (int8_t)q;
-    t -= q / sc[s];
+    t -= q;
   }
 }
 
-// max |B_x[m][n]| over n for every (x, m), as float bits (atomicMax on the
-// non-negative float's integer image); 32 x 32 (n, x) tiles through shared memory
-__global__ void __launch_bounds__(256) rowmax_kernel(const double* __restrict__ B, int64_t ldb,
-                                                     const int* __restrict__ rowmap, int nao,
-                                                     int64_t nfit, unsigned* __restrict__ rowmax) {
-  __shared__ float tile[32][33];
-  const int64_t n0 = (int64_t)blockIdx.x * 32, x0 = (int64_t)blockIdx.z * 32;
-  const int m = blockIdx.y;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int j = ty; j < 32; j += 8) {
-    const int64_t n = n0 + j, x = x0 + tx;
-    float v = 0.f;
-    if (n < nao && x < nfit) {
-      const int r = rowmap[(int64_t)m * nao + n];
-      if (r >= 0) v = (float)fabs(B[(int64_t)r * ldb + x]);
-    }
-    tile[j][tx] = v;
-  }
-  __syncthreads();
-  if (ty == 0) {
-    float mx = 0.f;
-    for (int j = 0; j < 32; ++j) mx = fmaxf(mx, tile[j][tx]);
-    const int64_t x = x0 + tx;
-    if (x < nfit && mx > 0.f) atomicMax(rowmax + x * nao + m, __float_as_uint(mx));
-  }
-}
-
-// int8 digit planes A[d][x][m][nao_p] and row exponents ea[x][m]
-__global__ void __launch_bounds__(256) digits_kernel(const double* __restrict__ B, int64_t ldb,
-                                                     const int* __restrict__ rowmap, int nao,
-                                                     int64_t nao_p, int64_t nfit,
-                                                     const unsigned* __restrict__ rowmax,
-                                                     int* __restrict__ ea, int64_t plane_bytes,
-                                                     int8_t* __restrict__ out) {
-  __shared__ double tile[32][33];
-  const int64_t n0 = (int64_t)blockIdx.x * 32, x0 = (int64_t)blockIdx.z * 32;
-  const int m = blockIdx.y;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int j = ty; j < 32; j += 8) {
-    const int64_t n = n0 + j, x = x0 + tx;
-    double v = 0.0;
-    if (n < nao && x < nfit) {
-      const int r = rowmap[(int64_t)m * nao + n];
-      if (r >= 0) v = B[(int64_t)r * ldb + x];
-    }
-    tile[j][tx] = v;
-  }
-  __syncthreads();
-  for (int j = ty; j < 32; j += 8) {
-    const int64_t x = x0 + j, n = n0 + tx;
-    if (x >= nfit || n >= nao_p) continue;
-    const int e = row_exponent((double)__uint_as_float(rowmax[x * nao + m]));
-    if (blockIdx.x == 0 && tx == 0) ea[x * nao + m] = e;
-    int8_t d[4];
-    digits4(tile[tx][j], e, d);
-    const int64_t o = (x * nao + m) * nao_p + n;
+// Digit planes of the square B_x: A[d][x][m][nao_p] (4 digits) with row
+// exponents ea[x][m], for XB fitted directions and one AO m per block. Row m
+// of B_x is gathered through m's list of (row of B, n) entries (both
+// triangles, screened pairs absent); pass 1 takes the row maxima, pass 2
+// (re-reading the same rows, now in L2) writes the digits into shared memory,
+// which then goes out as 16-byte stores. Loads are issued kU at a time per
+// thread so that the gathers overlap.
+template <int XB>
+__global__ void __launch_bounds__(256) kplanes_kernel(const double* __restrict__ B, int64_t ldb,
+                                                      const int* __restrict__ kptr,
+                                                      const int* __restrict__ krow,
+                                                      const int* __restrict__ kn, int nao,
+                                                      int64_t nao_p, int64_t nfit,
+                                                      int* __restrict__ ea, int64_t plane,
+                                                      int8_t* __restrict__ out) {
+  constexpr int G = 256 / XB;   // list entries in flight per block
+  constexpr int kU = 8;
+  extern __shared__ __align__(16) int8_t sd[];   // [4][XB][nao_p]
+  __shared__ double red[G][XB];
+  __shared__ int sh_e[XB];
+  const int m = blockIdx.x;
+  const int64_t x0 = (int64_t)blockIdx.y * XB;
+  const int lx = threadIdx.x % XB, g = threadIdx.x / XB;
+  const int64_t x = x0 + lx;
+  const bool xin = x < nfit;
+  const int e0 = kptr[m], e1 = kptr[m + 1];
+  double mx = 0.0;
+  if (xin) {
+    int e = e0 + g;
+    for (; e + (kU - 1) * G < e1; e += kU * G) {
+      int r[kU];
+      double v[kU];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) out[s * plane_bytes + o] = d[s];
+      for (int u = 0; u < kU; ++u) r[u] = krow[e + u * G];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) v[u] = B[(int64_t)r[u] * ldb + x];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) mx = fmax(mx, fabs(v[u]));
+    }
+    for (; e < e1; e += G) mx = fmax(mx, fabs(B[(int64_t)krow[e] * ldb + x]));
+  }
+  red[g][lx] = mx;
+  // zero the staging planes (screened n and the padding stay zero)
+  const int64_t nvec = 4 * XB * nao_p / 16;
+  for (int64_t q = threadIdx.x; q < nvec; q += 256) reinterpret_cast<int4*>(sd)[q] = make_int4(0, 0, 0, 0);
+  __syncthreads();
+  if (threadIdx.x < XB) {
+    double v = 0.0;
+    for (int j = 0; j < G; ++j) v = fmax(v, red[j][threadIdx.x]);
+    const int ex = row_exponent(v);
+    sh_e[threadIdx.x] = ex;
+    if (x0 + threadIdx.x < nfit) ea[(x0 + threadIdx.x) * nao + m] = ex;
+  }
+  __syncthreads();
+  const int ex = sh_e[lx];
+  if (xin) {
+    int e = e0 + g;
+    for (; e + (kU - 1) * G < e1; e += kU * G) {
+      int r[kU], n[kU];
+      double v[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        r[u] = krow[e + u * G];
+        n[u] = kn[e + u * G];
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) v[u] = B[(int64_t)r[u] * ldb + x];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        int8_t d[4];
+        digits<4>(v[u], ex, d);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) sd[((int64_t)s * XB + lx) * nao_p + n[u]] = d[s];
+      }
+    }
+    for (; e < e1; e += G) {
+      int8_t d[4];
+      digits<4>(B[(int64_t)krow[e] * ldb + x], ex, d);
+      const int n = kn[e];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) sd[((int64_t)s * XB + lx) * nao_p + n] = d[s];
+    }
+  }
+  __syncthreads();
+  const int64_t vrow = nao_p / 16;   // int4 per (digit, x) row
+  for (int64_t q = threadIdx.x; q < nvec; q += 256) {
+    const int64_t srow = q / vrow, c = q % vrow;
+    const int s = (int)(srow / XB), j = (int)(srow % XB);
+    if (x0 + j >= nfit) continue;
+    int8_t* dst = out + s * plane + ((x0 + j) * nao + m) * nao_p;
+    reinterpret_cast<int4*>(dst)[c] = reinterpret_cast<const int4*>(sd)[q];
   }
 }
 
-// digit planes of C^T: Ct[d][i][n] from Cp[n][i] (nao x nsel), exponents eb[i]
+// Digit planes of row-major rows with a per-row exponent: planes[d][row][kp]
+// (k < ncols from src[row * ld + k], zero up to kp), e_out[row]. One block per row.
+template <int ND>
+__global__ void __launch_bounds__(256) split_rows_kernel(const double* __restrict__ src, int64_t ld,
+                                                         int64_t ncols, int64_t kp,
+                                                         int* __restrict__ e_out,
+                                                         int64_t plane_stride,
+                                                         int8_t* __restrict__ planes) {
+  __shared__ double red[256];
+  const int64_t row = blockIdx.x;
+  const double* r = src + row * ld;
+  double mx = 0.0;
+  for (int64_t k = threadIdx.x; k < ncols; k += 256) mx = fmax(mx, fabs(r[k]));
+  red[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  const int e = row_exponent(red[0]);
+  if (threadIdx.x == 0) e_out[row] = e;
+  int8_t* dst = planes + row * kp;
+  for (int64_t k = threadIdx.x; k < kp; k += 256) {
+    int8_t d[ND] = {};
+    if (k < ncols) digits<ND>(r[k], e, d);
+#pragma unroll
+    for (int s = 0; s < ND; ++s) dst[s * plane_stride + k] = d[s];
+  }
+}
+
+// 4-digit planes of C'^T: Ct[d][i][n] from Cp[n][i] (nao x nsel), exponents eb[i]
 __global__ void __launch_bounds__(256) c_digits_kernel(const double* __restrict__ Cp, int nao,
                                                        int64_t nsel, int64_t nao_p,
                                                        int* __restrict__ eb,
@@ -120,7 +195,7 @@ __global__ void __launch_bounds__(256) c_digits_kernel(const double* __restrict_
   const int64_t plane = nsel * nao_p;
   for (int64_t n = threadIdx.x; n < nao_p; n += blockDim.x) {
     int8_t d[4] = {0, 0, 0, 0};
-    if (n < nao) digits4(Cp[n * nsel + i], e, d);
+    if (n < nao) digits<4>(Cp[n * nsel + i], e, d);
 #pragma unroll
     for (int s = 0; s < 4; ++s) out[s * plane + i * nao_p + n] = d[s];
   }
@@ -135,31 +210,93 @@ void check_oz_err(Plan& p, cudaStream_t s) {
 
 }  // namespace
 
-void build_ozaki_planes(Plan& p, cudaStream_t s) {
-  p.nao_p16 = (p.nao + 15) / 16 * 16;
-  const int64_t nfit = p.nfit, nao = p.nao;
-  const int64_t plane = nfit * nao * p.nao_p16;
-  p.d_oz_a.ensure((size_t)kOzDigits * plane);
-  p.d_oz_rowmax.ensure((size_t)nfit * nao * sizeof(unsigned));
-  p.d_oz_ea.ensure((size_t)nfit * nao * sizeof(int));
-  DFJK_CUDA(cudaMemsetAsync(p.d_oz_rowmax.p, 0, (size_t)nfit * nao * sizeof(unsigned), s));
-  const int64_t step = (int64_t)65535 * 32;
-  for (int64_t x0 = 0; x0 < nfit; x0 += step) {
-    const int64_t nx = std::min(step, nfit - x0);
-    dim3 grid((unsigned)((p.nao_p16 + 31) / 32), (unsigned)nao, (unsigned)((nx + 31) / 32));
-    rowmax_kernel<<<grid, 256, 0, s>>>(p.d_B.as<double>() + x0, p.ldb, p.d_rowmap.as<int>(), p.nao,
-                                       nx, p.d_oz_rowmax.as<unsigned>() + x0 * nao);
-    DFJK_LAUNCHED();
-    digits_kernel<<<grid, 256, 0, s>>>(p.d_B.as<double>() + x0, p.ldb, p.d_rowmap.as<int>(), p.nao,
-                                       p.nao_p16, nx, p.d_oz_rowmax.as<unsigned>() + x0 * nao,
-                                       p.d_oz_ea.as<int>() + x0 * nao, plane,
-                                       p.d_oz_a.as<int8_t>() + x0 * nao * p.nao_p16);
+template <int XB>
+static void launch_kplanes(Plan& p, int64_t plane, cudaStream_t s) {
+  const size_t smem = (size_t)4 * XB * p.nao_p16;
+  DFJK_CUDA(cudaFuncSetAttribute(kplanes_kernel<XB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  const int64_t nxb = (p.nfit + XB - 1) / XB;
+  for (int64_t b0 = 0; b0 < nxb; b0 += 65535) {
+    const int64_t nb = std::min<int64_t>(65535, nxb - b0);
+    const int64_t x0 = b0 * XB;
+    dim3 grid((unsigned)p.nao, (unsigned)nb);
+    kplanes_kernel<XB><<<grid, 256, smem, s>>>(
+        p.d_B.as<double>() + x0, p.ldb, p.d_kptr.as<int>(), p.d_krow.as<int>(), p.d_kn.as<int>(),
+        p.nao, p.nao_p16, p.nfit - x0, p.d_oz_ea.as<int>() + x0 * p.nao, plane,
+        p.d_oz_a.as<int8_t>() + x0 * p.nao * p.nao_p16);
     DFJK_LAUNCHED();
   }
 }
 
+void build_ozaki_planes(Plan& p, cudaStream_t s) {
+  p.nao_p16 = (p.nao + 15) / 16 * 16;
+  const int64_t nfit = p.nfit, nao = p.nao;
+  const int64_t plane = nfit * nao * p.nao_p16;
+  p.d_oz_a.ensure((size_t)kOzKDigits * plane);
+  p.d_oz_ea.ensure((size_t)nfit * nao * sizeof(int));
+  // 16 directions per block while the staging planes fit in 160 KB of shared memory
+  if ((size_t)4 * 16 * p.nao_p16 <= (size_t)160 << 10) launch_kplanes<16>(p, plane, s);
+  else if ((size_t)4 * 4 * p.nao_p16 <= (size_t)200 << 10) launch_kplanes<4>(p, plane, s);
+  else fail(DFJK_ERR_UNSUPPORTED, "mixed precision supports nao <= 12800");
+}
+
+void ozaki_prepare_l(Plan& p, cudaStream_t s) {
+  p.naux_p16 = (p.naux + 15) / 16 * 16;
+  const int64_t plane = p.ldb * p.naux_p16;
+  p.ws_oz_l.ensure((size_t)kOzBDigits * plane);
+  p.ws_oz_el.ensure((size_t)p.ldb * sizeof(int));
+  // L is column-major naux x ldb: column x (contiguous over P) is row x of L^T
+  split_rows_kernel<kOzBDigits><<<(unsigned)p.ldb, 256, 0, s>>>(
+      p.d_L.as<double>(), p.naux, p.naux, p.naux_p16, p.ws_oz_el.as<int>(), plane,
+      p.ws_oz_l.as<int8_t>());
+  DFJK_LAUNCHED();
+  p.ws_oz_err.ensure(sizeof(int));
+  DFJK_CUDA(cudaMemsetAsync(p.ws_oz_err.p, 0, sizeof(int), s));
+}
+
+// Bout[r][x] (ld ldb) = sum_P raw[r][P] L[P][x] for nr rows of raw (ld naux)
+void ozaki_bgemm(Plan& p, const double* raw, int64_t nr, double* Bout, cudaStream_t s) {
+  if (nr <= 0) return;
+  constexpr int ND = kOzBDigits;
+  const int bk = ozaki_box_k(ND);
+  const int64_t kp = p.naux_p16;
+  const int64_t plane = nr * kp;
+  p.ws_oz_raw.ensure((size_t)ND * plane);
+  p.ws_oz_er.ensure((size_t)nr * sizeof(int));
+  split_rows_kernel<ND><<<(unsigned)nr, 256, 0, s>>>(raw, p.naux, p.naux, kp, p.ws_oz_er.as<int>(),
+                                                     plane, p.ws_oz_raw.as<int8_t>());
+  DFJK_LAUNCHED();
+  OzakiMaps maps;
+  const int64_t lplane = p.ldb * kp;
+  for (int d = 0; d < ND; ++d)
+    ozaki_map(&maps.b[d], p.ws_oz_l.as<int8_t>() + d * lplane, p.naux, p.ldb, 1, kp, lplane, bk,
+              kOzBN);
+  OzakiArgs a{};
+  a.N = (int)p.ldb;
+  a.ktiles = (int)((p.naux + bk - 1) / bk);
+  a.plane0 = 0;
+  a.ea_stride = 0;
+  a.eb = p.ws_oz_el.as<int>();
+  a.ld_out = p.ldb;
+  a.batch_stride_out = 0;
+  a.err = p.ws_oz_err.as<int>();
+  // row blocks of at most 65535 * 128 rows (grid y)
+  const int64_t step = (int64_t)65535 * 128;
+  for (int64_t m0 = 0; m0 < nr; m0 += step) {
+    const int64_t mr = std::min(step, nr - m0);
+    for (int d = 0; d < ND; ++d)
+      ozaki_map(&maps.a[d], p.ws_oz_raw.as<int8_t>() + d * plane + m0 * kp, p.naux, mr, 1, kp, plane,
+                bk, 128);
+    a.M = (int)mr;
+    a.ea = p.ws_oz_er.as<int>() + m0;
+    a.out = Bout + m0 * p.ldb;
+    ozaki_launch(ND, maps, a, 1, s);
+  }
+  check_oz_err(p, s);
+}
+
 void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s) {
-  p.ws_oz_c.ensure((size_t)kOzDigits * nsel * p.nao_p16);
+  p.ws_oz_c.ensure((size_t)kOzKDigits * nsel * p.nao_p16);
   p.ws_oz_eb.ensure((size_t)nsel * sizeof(int));
   c_digits_kernel<<<(unsigned)nsel, 256, 0, s>>>(Cp, p.nao, nsel, p.nao_p16, p.ws_oz_eb.as<int>(),
                                                  p.ws_oz_c.as<int8_t>());
@@ -170,19 +307,21 @@ void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s) {
 
 // X[m][x - x0][i] (float64, ld n * nsel) for fitted directions [x0, x0 + n)
 void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStream_t s) {
+  constexpr int ND = kOzKDigits;
+  const int bk = ozaki_box_k(ND);
   const int64_t nao = p.nao, nao_p = p.nao_p16;
   const int64_t plane = p.nfit * nao * nao_p;
   OzakiMaps maps;
-  for (int d = 0; d < kOzDigits; ++d) {
+  for (int d = 0; d < ND; ++d) {
     ozaki_map(&maps.a[d], p.d_oz_a.as<int8_t>() + d * plane, nao, nao, p.nfit, nao_p, nao * nao_p,
-              128);
+              bk, 128);
     ozaki_map(&maps.b[d], p.ws_oz_c.as<int8_t>() + d * nsel * nao_p, nao, nsel, 1, nao_p,
-              nsel * nao_p, kOzBN);
+              nsel * nao_p, bk, kOzBN);
   }
   OzakiArgs a{};
   a.M = (int)nao;
   a.N = (int)nsel;
-  a.ktiles = (int)((nao + 127) / 128);
+  a.ktiles = (int)((nao + bk - 1) / bk);
   a.ea = p.d_oz_ea.as<int>();
   a.ea_stride = nao;
   a.eb = p.ws_oz_eb.as<int>();
@@ -194,7 +333,7 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
     const int64_t nz = std::min<int64_t>(65535, n - z0);
     a.plane0 = (int)(x0 + z0);
     a.out = X + z0 * nsel;
-    ozaki_launch(maps, a, (int)nz, s);
+    ozaki_launch(ND, maps, a, (int)nz, s);
   }
   check_oz_err(p, s);
 }

@@ -1,5 +1,5 @@
 // Exact-accumulation int8 tensor-core GEMM (tcgen05 kind::i8) for the
-// mixed-precision K half transform.
+// mixed-precision products of the DF path.
 #pragma once
 
 #include <cuda.h>
@@ -8,17 +8,19 @@
 
 namespace dfjk {
 
-constexpr int kOzDigits = 4;     // signed 7-bit digits per value (28 bits)
-constexpr int kOzBN = 80;        // n tile (occupied orbitals)
+constexpr int kOzBN = 80;          // n tile
+constexpr int kOzKDigits = 4;      // K half transform: 28 bits per value
+constexpr int kOzBDigits = 6;      // B = (ij|P) L: 42 bits per value (see ozaki.cu)
+constexpr int kOzMaxDigits = 6;
 
 struct OzakiMaps {
-  CUtensorMap a[kOzDigits];   // A digit planes, box (128 k, 128 rows, 1)
-  CUtensorMap b[kOzDigits];   // B digit planes, box (128 k, kOzBN rows, 1)
+  CUtensorMap a[kOzMaxDigits];   // A digit planes, box (k tile bytes, 128 rows, 1)
+  CUtensorMap b[kOzMaxDigits];   // B digit planes, box (k tile bytes, kOzBN rows, 1)
 };
 
 struct OzakiArgs {
   int M, N;                // output extent (rows of A, rows of B)
-  int ktiles;              // k tiles of 128
+  int ktiles;              // k tiles of ozaki_box_k(ndig) bytes
   int plane0;              // A plane of blockIdx.z == 0
   const int* ea;           // exponent per A row: ea[(plane0 + z) * ea_stride + row]
   int64_t ea_stride;
@@ -28,11 +30,16 @@ struct OzakiArgs {
   int* err;                // set non-zero when a bounded wait gives up
 };
 
-// 3-D int8 tensor map over [d2][d1][d0] (d0 contiguous; strides in bytes)
-void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
-               int64_t stride1, int64_t stride2, int box1);
+// k tile (bytes) of the kernel that runs ndig digits per value: 128 (4 digits,
+// 128-byte swizzle) or 64 (6 digits, 64-byte swizzle)
+int ozaki_box_k(int ndig);
 
-// grid (ceil(N/kOzBN), ceil(M/128), grid_z)
-void ozaki_launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s);
+// 3-D int8 tensor map over [d2][d1][d0] (d0 contiguous; strides in bytes),
+// box (box_k, box1, 1) with the swizzle that matches box_k
+void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
+               int64_t stride1, int64_t stride2, int box_k, int box1);
+
+// grid (ceil(N/kOzBN), ceil(M/128), grid_z); ndig is 4 or 6
+void ozaki_launch(int ndig, const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s);
 
 }  // namespace dfjk

@@ -1,23 +1,26 @@
 // Exact-accumulation int8 GEMM on the 5th-generation tensor cores.
 //
 //   D[m][n] = 2^(ea[m] + eb[n]) * sum_k a[m][k] b[n][k]
-// where every value is stored as four signed 7-bit digits under its row's
+// where every value is stored as ND signed 7-bit digits under its row's
 // exponent: a = 2^ea * sum_s d_s 2^(-7(s+1)), |d_s| <= 64 (Ozaki-style
-// splitting). The ten digit products of combined order o = s + t <= 3 are
-// accumulated EXACTLY in int32 (kind::i8 MMA), one tensor-memory accumulator
-// per order; the epilogue combines them in float64 with weights 2^(-7(o+2)).
-// The only error is the truncation of the digit expansion (2^-27 of the row
-// maximum); unlike fp32 accumulation there is no rounding drift with k.
-// (Float32 accumulation of split-bf16 products was measured to bias K toward
-// zero by ~1e-6 per 24 MMAs, growing with the k length; that path was dropped.)
+// splitting). The ND(ND+1)/2 digit products of combined order o = s + t < ND
+// are accumulated EXACTLY in int32 (kind::i8 MMA), one tensor-memory
+// accumulator per order; the epilogue combines them in float64 with weights
+// 2^(-7(o+2)). The only error is the truncation of the digit expansion
+// (2^(1-7ND) of the row maximum); unlike fp32 accumulation there is no
+// rounding drift with k. (Float32 accumulation of split-bf16 products was
+// measured to bias K toward zero by ~1e-6 per 24 MMAs, growing with the k
+// length; that path was dropped.)
 //
-// Tiles: 128 (m) x 80 (n) x 128 (k, bytes), K-major operands, TMA with the
-// 128-byte swizzle into a 2-stage mbarrier ring (4 digit planes per operand
-// per stage, 104 KB). Warp 0 lane 0 issues copies, warp 1 lane 0 issues MMAs
-// (4 per k tile per digit pair), all four warps drain tensor memory
-// (warp w owns rows 32w..32w+31). Every wait is bounded (4 s of
-// %globaltimer); a timeout sets *err, skips the remaining work, drains the
-// copies in flight (bounded) and still frees the tensor memory.
+// Tiles: 128 (m) x 80 (n) x BK (k, bytes), K-major operands, TMA with the
+// BK-byte swizzle into an mbarrier ring (ND digit planes per operand per
+// stage). Two shapes are compiled: ND 4 with BK 128 (104 KB stages) and ND 6
+// with BK 64 (78 KB stages), both double-buffered. Warp 0 lane 0 issues
+// copies, warp 1 lane 0 issues MMAs (BK/32 per digit pair per k tile), all
+// four warps drain tensor memory (warp w owns rows 32w..32w+31). Every wait
+// is bounded (4 s of %globaltimer); a timeout sets *err, skips the remaining
+// work, drains the copies in flight (bounded) and still frees the tensor
+// memory.
 #include "ozaki.h"
 
 #include <mutex>
@@ -26,8 +29,8 @@ namespace dfjk {
 
 namespace {
 
-constexpr int kBM = 128, kBK = 128, kStages = 2, kD = kOzDigits, kBN = kOzBN;
-constexpr uint32_t kTmemCols = 512;        // 4 order accumulators at 128-column stride
+constexpr int kBM = 128, kBN = kOzBN, kStages = 2;
+constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kWaitNs = 4000000000ull;
 
 __device__ __forceinline__ uint64_t now_ns() {
@@ -84,14 +87,17 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
-// K-major, 128-byte swizzle: 8-row atoms of 1024 B (SBO), 16 B leading
-// offset, descriptor version 1 (sm_100)
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// K-major shared-memory descriptor (sm_100, version 1) for BK-byte rows with
+// the BK-byte swizzle: 8-row atoms of 8 * BK bytes (SBO), leading offset
+// unused (1); layout type 2 = 128-byte swizzle, 4 = 64-byte swizzle
+template <int BK>
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t saddr) {
+  static_assert(BK == 128 || BK == 64, "k tile must be 64 or 128 bytes");
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
   d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)((8 * BK) >> 4) << 32;
   d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;
+  d |= (uint64_t)(BK == 128 ? 2 : 4) << 61;
   return d;
 }
 
@@ -111,7 +117,7 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int (&v)[16]) {
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v) {
   uint32_t r[16];
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
@@ -125,11 +131,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
 }
 
+template <int ND, int BK>
 __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ OzakiMaps maps,
                                                         OzakiArgs a) {
-  constexpr uint32_t A_TILE = kBM * kBK;   // 16 KB
-  constexpr uint32_t B_TILE = kBN * kBK;   // 10 KB
-  constexpr uint32_t STAGE = kD * (A_TILE + B_TILE);
+  constexpr uint32_t A_TILE = kBM * BK;
+  constexpr uint32_t B_TILE = kBN * BK;
+  constexpr uint32_t STAGE = ND * (A_TILE + B_TILE);
+  constexpr int KSTEPS = BK / 32;   // one kind::i8 MMA covers 32 bytes of k
+  // accumulator o at column o * ACC (128 when they fit, else packed at kBN)
+  constexpr uint32_t ACC = (ND * 128 <= (int)kTmemCols) ? 128 : kBN;
+  static_assert(ND * ACC <= kTmemCols, "order accumulators exceed tensor memory");
+  static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles must keep 1 KB alignment");
   // S32 accumulator (c_format 2), signed int8 A and B (format 1), N>>3, M>>4
   constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
                              ((uint32_t)(kBM >> 4) << 24);
@@ -174,9 +186,9 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
       mbar_expect_tx(full, STAGE);
       uint8_t* st = smem + s * STAGE;
 #pragma unroll
-      for (int d = 0; d < kD; ++d) {
-        tma_load_3d(smem_u32(st + d * A_TILE), &maps.a[d], full, i * kBK, m0, a.plane0 + z);
-        tma_load_3d(smem_u32(st + kD * A_TILE + d * B_TILE), &maps.b[d], full, i * kBK, n0, 0);
+      for (int d = 0; d < ND; ++d) {
+        tma_load_3d(smem_u32(st + d * A_TILE), &maps.a[d], full, i * BK, m0, a.plane0 + z);
+        tma_load_3d(smem_u32(st + ND * A_TILE + d * B_TILE), &maps.b[d], full, i * BK, n0, 0);
       }
       ++issued;
     }
@@ -189,27 +201,26 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
     }
   } else if (threadIdx.x == 32 && nk > 0) {
     bool ok = true;
-    // digit pairs (s, t) with s + t <= 3, and their order accumulator
-    const int pa[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
-    const int pb[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
-    const int po[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
-    const int first[10] = {1, 1, 0, 1, 0, 0, 1, 0, 0, 0};   // first pair of its order
     for (int i = 0; i < nk; ++i) {
       const int s = i % kStages;
       ok = mbar_wait(smem_u32(&bars[s]), (i / kStages) & 1, a.err, 2);
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t base = smem_u32(smem + s * STAGE);
-      const uint32_t bbase = base + kD * A_TILE;
+      const uint32_t bbase = base + ND * A_TILE;
+      // digit pairs (sa, o - sa) of order o into accumulator o
 #pragma unroll
-      for (int t = 0; t < 10; ++t) {
-        const uint64_t ad = sw128_desc(base + pa[t] * A_TILE);
-        const uint64_t bd = sw128_desc(bbase + pb[t] * B_TILE);
-        const uint32_t dcol = tmem + (uint32_t)(po[t] * 128);
+      for (int o = 0; o < ND; ++o) {
+        const uint32_t dcol = tmem + (uint32_t)o * ACC;
 #pragma unroll
-        for (int k = 0; k < kBK / 32; ++k)
-          umma_i8(dcol, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), IDESC,
-                  (i > 0 || !first[t] || k > 0) ? 1u : 0u);
+        for (int sa = 0; sa <= o; ++sa) {
+          const uint64_t ad = kmajor_desc<BK>(base + sa * A_TILE);
+          const uint64_t bd = kmajor_desc<BK>(bbase + (o - sa) * B_TILE);
+#pragma unroll
+          for (int k = 0; k < KSTEPS; ++k)
+            umma_i8(dcol, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), IDESC,
+                    (i > 0 || sa > 0 || k > 0) ? 1u : 0u);
+        }
       }
       umma_commit(smem_u32(&bars[kStages + s]));
     }
@@ -226,20 +237,19 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
     const int era = row < a.M ? a.ea[(int64_t)(a.plane0 + z) * a.ea_stride + row] : 0;
     double* orow = a.out + (int64_t)z * a.batch_stride_out + (int64_t)row * a.ld_out;
     for (int c = 0; c < kBN; c += 16) {
-      int v0[16], v1[16], v2[16], v3[16];
-      tmem_ld16(trow + c, v0);
-      tmem_ld16(trow + 128 + c, v1);
-      tmem_ld16(trow + 256 + c, v2);
-      tmem_ld16(trow + 384 + c, v3);
+      int v[ND][16];
+#pragma unroll
+      for (int o = 0; o < ND; ++o) tmem_ld16(trow + (uint32_t)o * ACC + c, v[o]);
       if (row >= a.M) continue;
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int col = n0 + c + j;
         if (col >= a.N) break;
-        // sum_o acc_o 2^(-7(o+2)), exact in float64 up to the final rounding
-        const double v = (double)v0[j] * 0x1p-14 + (double)v1[j] * 0x1p-21 +
-                         (double)v2[j] * 0x1p-28 + (double)v3[j] * 0x1p-35;
-        orow[col] = ldexp(v, era + a.eb[col]);
+        // sum_o acc_o 2^(-7(o+2)), highest order first
+        double t = 0.0;
+#pragma unroll
+        for (int o = ND - 1; o >= 0; --o) t = t * 0x1p-7 + (double)v[o][j];
+        orow[col] = ldexp(t, era + a.eb[col] - 14);
       }
     }
   }
@@ -270,32 +280,47 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-constexpr size_t kSmem = kStages * (size_t)kD * (kBM * kBK + kBN * kBK) + 1024 + 256;
+template <int ND, int BK>
+constexpr size_t smem_bytes() {
+  return (size_t)kStages * ND * (kBM * BK + kBN * BK) + 1024 + 256;
+}
+
+template <int ND, int BK>
+void launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
+  constexpr size_t smem = smem_bytes<ND, BK>();
+  static_assert(smem <= 232448, "stages exceed the shared memory of one CTA");
+  dim3 grid((a.N + kBN - 1) / kBN, (a.M + kBM - 1) / kBM, grid_z);
+  DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8<ND, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  ozaki_gemm_i8<ND, BK><<<grid, 128, smem, s>>>(maps, a);
+  DFJK_LAUNCHED();
+}
 
 }  // namespace
 
+int ozaki_box_k(int ndig) { return ndig == 6 ? 64 : 128; }
+
 void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
-               int64_t stride1, int64_t stride2, int box1) {
+               int64_t stride1, int64_t stride2, int box_k, int box1) {
   if ((reinterpret_cast<uintptr_t>(base) & 15) || (stride1 % 16) || (stride2 % 16))
     fail(DFJK_ERR_INVALID, "tensor map: base or strides not 16-byte aligned");
+  if (box_k != 64 && box_k != 128) fail(DFJK_ERR_INVALID, "tensor map: k box must be 64 or 128");
   cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
   cuuint64_t strides[2] = {(cuuint64_t)stride1, (cuuint64_t)stride2};
-  cuuint32_t box[3] = {(cuuint32_t)kBK, (cuuint32_t)box1, 1};
+  cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box1, 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims,
                            strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                           box_k == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) fail(DFJK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
 
-void ozaki_launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
+void ozaki_launch(int ndig, const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
   if (grid_z <= 0 || a.M <= 0 || a.N <= 0) return;
-  dim3 grid((a.N + kBN - 1) / kBN, (a.M + kBM - 1) / kBM, grid_z);
-  DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmem));
-  ozaki_gemm_i8<<<grid, 128, kSmem, s>>>(maps, a);
-  DFJK_LAUNCHED();
+  if (ndig == 4) launch<4, 128>(maps, a, grid_z, s);
+  else if (ndig == 6) launch<6, 64>(maps, a, grid_z, s);
+  else fail(DFJK_ERR_INVALID, "unsupported digit count %d", ndig);
 }
 
 }  // namespace dfjk

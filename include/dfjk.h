@@ -39,9 +39,10 @@ typedef enum {
 /* Precision of the build and contractions. */
 enum {
   DFJK_FP64 = 0,  /* float64 integrals, B, J and K                               */
-  DFJK_MIXED = 1  /* float64 integrals, B and J; the K half transform on int8
-                     tensor cores (4 digits per value, exact int32 accumulation),
-                     extra 4*nfit*nao^2 bytes of device memory                  */
+  DFJK_MIXED = 1  /* float64 integrals, metric, stored B and J; the products
+                     B = (ij|P) L and B_x C on int8 tensor cores (4 digits per
+                     value, exact int32 accumulation, float64 epilogue); extra
+                     4*nfit*nao^2 bytes of device memory                        */
 };
 
 /* Basis arrays in dftax's BasisData layout (dftax/energy/gto.py:132-156):
@@ -146,7 +147,8 @@ enum {
   DFJK_PHASE_J = 4,      /* gamma and J                                       */
   DFJK_PHASE_KHALF = 5,  /* K half transform                                  */
   DFJK_PHASE_KSYRK = 6,  /* K accumulation                                    */
-  DFJK_PHASE_COUNT = 7
+  DFJK_PHASE_KPLANES = 7, /* mixed precision: int8 digit planes of B for K    */
+  DFJK_PHASE_COUNT = 8
 };
 
 /* Milliseconds per phase of the last build / J-K call: ms[0..n). Synchronizes
