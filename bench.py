@@ -7,8 +7,14 @@ orbitals, seeded geometry and C_occ): the (P|Q) metric and its factor, the
 arrays, C) are resident before the timed region; B (16.7 GB in float64) is
 larger than L2, so no explicit flush is needed between steps.
 
+The headline (``--precision both``, the default) is the mixed-precision form
+(int8 tensor-core products with exact accumulation; integrals, metric and J
+in float64); the float64 form of the same step is timed in the same run and
+reported under ``fp64``, with |dE|, max|dJ| and max|dK| of the mixed result
+against it under ``accuracy_vs_fp64``.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload water32] [--precision fp64|mixed]
+                    [--workload water32] [--precision both|mixed|fp64]
 
 N > 1 runs under torchrun, one rank per GPU; each rank builds its own cluster
 (seeded by rank): the path has no exchange between molecules, so the ranks are
@@ -43,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="water32")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -227,6 +233,48 @@ def load_traffic(kernel: str, workload: str):
     return d.get(f"{kernel}@{workload}")
 
 
+def int8_gemm_peak(torch):
+    """Burst int8 tensor-core GEMM rate (torch._int_mm, cuBLASLt, 8192^3, best of 5) in TOP/s."""
+    n = 8192
+    try:
+        a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device="cuda")
+        b = torch.randint(-64, 64, (n, n), dtype=torch.int8, device="cuda")
+        for _ in range(2):
+            torch._int_mm(a, b)
+        best = 1e30
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12, "in-bench cuBLASLt int8 GEMM 8192^3 burst"
+    except Exception as ex:  # pragma: no cover - depends on the cuBLASLt build
+        _, bf16, src = measured_peaks()
+        return 2.0 * bf16, f"2 x {src} bf16 (int8 GEMM unavailable: {type(ex).__name__})"
+
+
+def timed_steps(torch, step, steps, warmup, stream, barrier, lib):
+    """W untimed steps, then K steps between CUDA events on the launching stream."""
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    l0 = lib.dfjk_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    return e0.elapsed_time(e1), (lib.dfjk_kernel_launches() - l0) // max(steps, 1)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -246,56 +294,52 @@ def run_ours(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    head = "mixed" if args.precision in ("both", "mixed") else "fp64"
+    precs = [head] + (["fp64"] if args.precision == "both" else [])
     sym, xyz, orb, aux, nocc = systems.workload(args.workload, seed=rank)
     C = systems.random_occupied(orb.nao, nocc, seed=100 + rank)
-    plan = Plan(orb, aux, precision=args.precision)
     Cd = torch.as_tensor(C, device="cuda")
-    J = torch.empty((orb.nao, orb.nao), dtype=torch.float64, device="cuda")
-    K = torch.empty_like(J)
     stream = torch.cuda.current_stream()
-
-    def step():
-        plan.build(stream)
-        plan.jk(Cd, out=(J, K), stream=stream)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
     lib = _lib.load()
-    clocks = Clocks(local_rank)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    l0 = lib.dfjk_kernel_launches()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    launches = (lib.dfjk_kernel_launches() - l0) // args.steps
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    phases = plan.phase_times()
-    info = plan.info()
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_step = ms / args.steps
-    value = world * args.steps / (ms / 1e3)
+    res = {}
+    for prec in precs:
+        plan = Plan(orb, aux, precision=prec)
+        J = torch.empty((orb.nao, orb.nao), dtype=torch.float64, device="cuda")
+        K = torch.empty_like(J)
 
-    # per-iteration J/K with B resident (the SCF inner loop)
-    nit = 5
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(nit):
-        plan.jk(Cd, out=(J, K), stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    jk_ms = e0.elapsed_time(e1) / nit
-    jk_phases = plan.phase_times()
+        def step():
+            plan.build(stream)
+            plan.jk(Cd, out=(J, K), stream=stream)
+
+        clocks = Clocks(local_rank)
+        clocks.start()
+        ms, launches = timed_steps(torch, step, args.steps, args.warmup, stream, barrier, lib)
+        clk = clocks.stop()
+        ms = max_over_ranks(ms)
+        phases = plan.phase_times()
+        # per-iteration J/K with B resident (the SCF inner loop)
+        jk_ms, _ = timed_steps(torch, lambda: plan.jk(Cd, out=(J, K), stream=stream), 5, 1, stream,
+                               barrier, lib)
+        jk_phases = plan.phase_times()
+        P = 2.0 * Cd @ Cd.T
+        e, _ = plan.energy(P, 0.25, want_grad=False, stream=stream)
+        res[prec] = {"ms": ms, "launches": launches, "clocks": clk, "phases": phases,
+                     "jk_ms": max_over_ranks(jk_ms / 5), "jk_phases": jk_phases, "info": plan.info(),
+                     "J": J.cpu().numpy(), "K": K.cpu().numpy(), "E": e}
+        plan.close()
+        del plan, J, K
+        torch.cuda.empty_cache()
+
+    r = res[head]
+    info = r["info"]
+    value = world * args.steps / (r["ms"] / 1e3)
 
     # end to end through the public host API: host basis arrays and C in,
     # host J and K out, copies inside the timed region
@@ -304,67 +348,96 @@ def run_ours(args, rank, world, local_rank):
     h2d = sum(a.nbytes for b in (orb, aux) for a in (b.centers, b.exponents, b.coefficients,
                                                       b.angular, b.cart2sph)) + C.nbytes
     d2h = Jh.nbytes + Kh.nbytes
-    del plan
     torch.cuda.synchronize()
     barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.e2e_steps):
-        p2 = Plan(orb, aux, precision=args.precision)
+        p2 = Plan(orb, aux, precision=head)
         p2.build(stream)
         p2.jk_host(C, J=Jh, K=Kh, stream=stream)
         p2.close()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = world * args.e2e_steps / (e2e_ms / 1e3)
 
-    # roofline of the dominant phase
+    # roofline of the dominant phase of the headline precision
     hbm, bf16, src = measured_peaks()
     fp64 = fp64_gemm_peak(torch) if rank == 0 else None
+    i8, i8_src = int8_gemm_peak(torch) if rank == 0 else (None, "")
     nrows, naux, nfit, nao = info["nrows"], info["naux"], info["nfit"], info["nao"]
     ldb = (nfit + 7) // 8 * 8
+    nao_p = (nao + 15) // 16 * 16
+    mixed = head == "mixed"
     units = {
-        "eri3c": ("hbm", 8.0 * nrows * naux / 1e9, "GB/s", hbm, "bytes of (ij|P) rows written"),
-        "bgemm": ("fp64", 2.0 * nrows * naux * ldb / 1e12, "TFLOP/s", fp64, "2 nrows naux nfit"),
-        "j": ("hbm", 2.0 * 8.0 * nrows * ldb / 1e9, "GB/s", hbm, "B streamed twice"),
-        "khalf": ("fp64", 2.0 * (2 * nrows - nao) * nfit * nocc / 1e12, "TFLOP/s", fp64,
-                  "2 sum_m |list(m)| nfit nocc"),
+        "eri3c": ("hbm", 8.0 * nrows * naux / 1e9, "GB/s", hbm, f"{src} hbm_gbs",
+                  "bytes of (ij|P) rows written"),
+        "j": ("hbm", 2.0 * 8.0 * nrows * ldb / 1e9, "GB/s", hbm, f"{src} hbm_gbs",
+              "B streamed twice"),
         "ksyrk": ("fp64", 1.0 * nao * (nao + 1) * nfit * nocc / 1e12, "TFLOP/s", fp64,
-                  "nao (nao+1) nfit nocc"),
+                  "in-bench cuBLAS DGEMM 8192^3 burst", "nao (nao+1) nfit nocc"),
     }
-    dom = max((k for k in units), key=lambda k: phases.get(k, 0.0))
-    bound, amount, unit, peak, what = units[dom]
+    if mixed:
+        units["bgemm"] = ("tensor", 21 * 2.0 * nrows * naux * nfit / 1e12, "TOP/s", i8, i8_src,
+                          "int8 ops: 21 digit products x 2 nrows naux nfit")
+        units["khalf"] = ("tensor", 10 * 2.0 * nfit * nao * nao * nocc / 1e12, "TOP/s", i8, i8_src,
+                          "int8 ops: 10 digit products x 2 nfit nao^2 nocc")
+        units["kplanes"] = ("hbm", (2 * 8.0 * (2 * nrows - nao) * nfit + 4.0 * nfit * nao * nao_p) / 1e9,
+                            "GB/s", hbm, f"{src} hbm_gbs",
+                            "B gathered twice per AO list + 4 int8 digit planes written")
+    else:
+        units["bgemm"] = ("fp64", 2.0 * nrows * naux * ldb / 1e12, "TFLOP/s", fp64,
+                          "in-bench cuBLAS DGEMM 8192^3 burst", "2 nrows naux nfit")
+        units["khalf"] = ("fp64", 2.0 * (2 * nrows - nao) * nfit * nocc / 1e12, "TFLOP/s", fp64,
+                          "in-bench cuBLAS DGEMM 8192^3 burst", "2 sum_m |list(m)| nfit nocc")
+    phases = {k: v for k, v in r["phases"].items() if k not in ("j", "khalf", "ksyrk")}
+    phases |= {k: r["jk_phases"][k] for k in ("j", "khalf", "ksyrk")}
+    dom = max(units, key=lambda k: phases.get(k, 0.0))
+    bound, amount, unit, peak, peak_src, what = units[dom]
     achieved = amount / (phases[dom] / 1e3) if phases[dom] > 0 else 0.0
-    roof = {"kernel": dom, "bound": "hbm" if bound == "hbm" else "fp64",
+    roof = {"kernel": dom, "bound": "hbm" if bound == "hbm" else bound,
             "achieved": round(achieved, 3), "peak": round(peak, 3) if peak else None, "unit": unit,
-            "frac": round(achieved / peak, 4) if peak else None,
-            "peak_source": (f"{src} hbm_gbs" if bound == "hbm" else "in-bench cuBLAS DGEMM 8192^3 burst"),
+            "frac": round(achieved / peak, 4) if peak else None, "peak_source": peak_src,
             "algorithmic": what, "ms_per_launch_group": round(phases[dom], 3),
-            "traffic": load_traffic(dom, args.workload)}
+            "traffic": load_traffic(dom + ("@mixed" if mixed else ""), args.workload)}
 
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms"] / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32+bf16x3", "data": "synthetic",
+        "dtype": "f64+i8" if mixed else "f64", "data": "synthetic",
         "config": {"workload": f"{args.workload} one DF J/K build from geometry (seeded)",
                    "nao": nao, "naux": naux, "nocc": nocc, "nfit": nfit, "nrows": nrows,
-                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "precision": head, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (B is %.1f GB)" % (8.0 * nrows * ldb / 1e9)},
-        "phases_ms": {k: round(v, 3) for k, v in phases.items() if k not in ("j", "khalf", "ksyrk")}
-        | {k: round(jk_phases[k], 3) for k in ("j", "khalf", "ksyrk")},
-        "jk_iteration": {"value": round(1e3 / jk_ms, 3), "unit": "J/K builds/s with B resident",
-                         "ms": round(jk_ms, 3)},
+        "phases_ms": {k: round(v, 3) for k, v in phases.items()},
+        "jk_iteration": {"value": round(1e3 / r["jk_ms"], 3), "unit": "J/K builds/s with B resident",
+                         "ms": round(r["jk_ms"], 3)},
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": int(launches),
+        "gpu_launches": int(r["launches"]),
         "roofline": roof,
-        "clocks": clk,
+        "clocks": r["clocks"],
     }
+    if "fp64" in res and head != "fp64":
+        f = res["fp64"]
+        line["fp64"] = {"value": round(world * args.steps / (f["ms"] / 1e3), 4), "unit": UNIT,
+                        "ms_per_step": round(f["ms"] / args.steps, 3),
+                        "jk_iteration_ms": round(f["jk_ms"], 3),
+                        "phases_ms": {k: round(v, 3) for k, v in f["phases"].items()
+                                      if k not in ("j", "khalf", "ksyrk", "kplanes")}
+                        | {k: round(f["jk_phases"][k], 3) for k in ("j", "khalf", "ksyrk")},
+                        "clocks": f["clocks"], "gpu_launches": int(f["launches"])}
+        line["speedup_vs_fp64"] = {"build_and_jk": round(f["ms"] / r["ms"], 3),
+                                   "jk_iteration": round(f["jk_ms"] / r["jk_ms"], 3)}
+        line["accuracy_vs_fp64"] = {
+            "abs_dE_Ha": abs(r["E"] - f["E"]), "E_fp64_Ha": f["E"],
+            "max_abs_dJ": float(np.abs(r["J"] - f["J"]).max()),
+            "max_abs_dK": float(np.abs(r["K"] - f["K"]).max()),
+            "rel_dJ": float(np.linalg.norm(r["J"] - f["J"]) / np.linalg.norm(f["J"])),
+            "rel_dK": float(np.linalg.norm(r["K"] - f["K"]) / np.linalg.norm(f["K"])),
+            "energy": "DFCoulomb energy of P = 2 C C^T with a_x = 0.25 (PBE0 exchange share)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, parts, sample = cpu_build_seconds(args.workload)
         line["cpu_baseline"] = {"value": round(1.0 / sec, 6), "unit": UNIT, "cores": cpu_cores(),
