@@ -205,6 +205,8 @@ struct Plan {
   DevBuf ws_oz_c, ws_oz_eb, ws_oz_err;
   // mixed precision: digit planes of L^T (per build) and of one raw 3-center chunk
   DevBuf ws_oz_l, ws_oz_el, ws_oz_raw, ws_oz_er;
+  // mixed precision: digit slices of X, their exponents and per-slice K partials
+  DevBuf ws_oz_x, ws_oz_ex, ws_oz_kp;
 };
 
 // ---- mixed precision on the int8 tensor cores (ozaki.cu) ----
@@ -213,6 +215,8 @@ void ozaki_bgemm(Plan& p, const double* raw, int64_t nr, double* Bout, cudaStrea
 void build_ozaki_planes(Plan& p, cudaStream_t s);
 void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s);
 void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStream_t s);
+void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, double* K,
+                cudaStream_t s);
 
 // ---- kernels & launchers (md.cu) ----
 void boys_table_host(std::vector<double>& tbl, std::vector<double>& asym);

@@ -281,10 +281,15 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
     }
     p.timer.mark(kPhKhalf, s);
     p.timer.mark(kPhKsyrk, s);
-    // X row-major (nao x n*nsel) == column-major (n*nsel x nao): K = op(A) op(A)^T, op = T
-    const double alpha = sign, beta = beta0 ? 0.0 : 1.0;
-    DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)nao, (int)(n * nsel),
-                            &alpha, X.as<double>(), (int)(n * nsel), &beta, K, (int)nao));
+    if (p.opts.precision == DFJK_MIXED) {
+      ozaki_syrk(p, X.as<double>(), n * nsel, sign, beta0, K, s);   // full square, int8 tensor cores
+    } else {
+      // X row-major (nao x n*nsel) == column-major (n*nsel x nao): K = op(A) op(A)^T, op = T
+      const double alpha = sign, beta = beta0 ? 0.0 : 1.0;
+      DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)nao,
+                              (int)(n * nsel), &alpha, X.as<double>(), (int)(n * nsel), &beta, K,
+                              (int)nao));
+    }
     p.timer.mark(kPhKsyrk, s);
     beta0 = false;
   }

@@ -1,10 +1,11 @@
-// Mixed precision (precision = DFJK_MIXED): the two large products of the DF
+// Mixed precision (precision = DFJK_MIXED): the three large products of the DF
 // path on the int8 tensor cores with exact accumulation (ozaki_gemm.cu):
 //   B[r][x] = sum_P (ij|P)[r][P] L[P][x]      (build, per raw row chunk)
 //   X[m][x][i] = sum_n B_x[m][n] C'[n][i]     (K half transform, per call)
+//   K[m][n] = sum_(x,i) X[m][x][i] X[n][x][i]  (K accumulation, per call)
 // Both operands of each product are split into signed 7-bit digits under a
-// per-row exponent; outputs are float64, and J, the metric, its factor L and
-// the K accumulation X X^T stay float64.
+// per-row exponent; outputs are float64. The integrals, the metric, its
+// factor L, the stored B and J stay float64.
 //
 // Accuracy findings behind the digit counts (device runs on water clusters,
 // against the float64 path of the same plan):
@@ -21,7 +22,10 @@
 //     eigenvalues cancel the smooth part of each (ij|P) row, which amplifies
 //     the truncation by up to the metric's condition number. With 4 digits,
 //     E moved by 1.5e-5 Ha for (H2O)_8 and 1.0e-4 Ha for (H2O)_32, so the
-//     build uses 6 digits (2^-41), 2^14 times finer.
+//     build uses 6 digits (2^-41), 2^14 times finer;
+//   * K = X X^T sums nfit * nocc products per element, with strong
+//     cancellation off the diagonal: with 4 digits K moved by 2.9e-7 relative
+//     and E by 3.1e-6 Ha for (H2O)_32, so it uses 5 digits (2^-34).
 #include "ozaki.h"
 
 #include <algorithm>
@@ -173,6 +177,48 @@ __global__ void __launch_bounds__(256) split_rows_kernel(const double* __restric
 #pragma unroll
     for (int s = 0; s < ND; ++s) dst[s * plane_stride + k] = d[s];
   }
+}
+
+// ND-digit planes of k slices of a row-major matrix X (nrows x kt, ld kt):
+// planes[d][z][row][ks] for slice z = blockIdx.y (zero past kt), one exponent
+// per (slice, row): e_out[z * nrows + row]. One block per (row, slice).
+template <int ND>
+__global__ void __launch_bounds__(256) split_slices_kernel(const double* __restrict__ X, int64_t kt,
+                                                           int64_t nrows, int64_t ks,
+                                                           int* __restrict__ e_out, int64_t plane,
+                                                           int8_t* __restrict__ planes) {
+  __shared__ double red[256];
+  const int64_t row = blockIdx.x, z = blockIdx.y;
+  const int64_t k0 = z * ks;
+  const int64_t nk = kt - k0 < ks ? kt - k0 : ks;
+  const double* r = X + row * kt + k0;
+  double mx = 0.0;
+  for (int64_t k = threadIdx.x; k < nk; k += 256) mx = fmax(mx, fabs(r[k]));
+  red[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  const int e = row_exponent(red[0]);
+  if (threadIdx.x == 0) e_out[z * nrows + row] = e;
+  int8_t* dst = planes + (z * nrows + row) * ks;
+  for (int64_t k = threadIdx.x; k < ks; k += 256) {
+    int8_t d[ND] = {};
+    if (k < nk) digits<ND>(r[k], e, d);
+#pragma unroll
+    for (int s = 0; s < ND; ++s) dst[s * plane + k] = d[s];
+  }
+}
+
+// K[i] = (beta0 ? 0 : K[i]) + sign * sum_z part[z][i], z in a fixed order
+__global__ void reduce_slices_kernel(const double* __restrict__ part, int64_t nslice, int64_t n,
+                                     double sign, int beta0, double* __restrict__ K) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc = 0.0;
+  for (int64_t z = 0; z < nslice; ++z) acc += part[z * n + i];
+  K[i] = beta0 ? sign * acc : K[i] + sign * acc;
 }
 
 // 4-digit planes of C'^T: Ct[d][i][n] from Cp[n][i] (nao x nsel), exponents eb[i]
@@ -335,6 +381,55 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
     a.out = X + z0 * nsel;
     ozaki_launch(ND, maps, a, (int)nz, s);
   }
+  check_oz_err(p, s);
+}
+
+// K (+)= sign * X X^T for one chunk of X (nao x kt, row-major): k in slices of
+// kOzSlice bytes, each with its own row exponents and its own float64 partial
+// (full square, exactly symmetric: both triangles come from the same integer
+// sums), then summed in a fixed order, so K is bit-reproducible.
+void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, double* K,
+                cudaStream_t s) {
+  constexpr int ND = kOzSDigits;
+  constexpr int64_t KS = kOzSlice;
+  const int bk = ozaki_box_k(ND);
+  const int64_t nao = p.nao;
+  const int64_t nsl = (kt + KS - 1) / KS;
+  const int64_t plane = nsl * nao * KS;
+  p.ws_oz_x.ensure((size_t)ND * plane);
+  p.ws_oz_ex.ensure((size_t)nsl * nao * sizeof(int));
+  p.ws_oz_kp.ensure((size_t)nsl * nao * nao * sizeof(double));
+  split_slices_kernel<ND><<<dim3((unsigned)nao, (unsigned)nsl), 256, 0, s>>>(
+      X, kt, nao, KS, p.ws_oz_ex.as<int>(), plane, p.ws_oz_x.as<int8_t>());
+  DFJK_LAUNCHED();
+  OzakiMaps maps;
+  for (int d = 0; d < ND; ++d) {
+    const int8_t* base = p.ws_oz_x.as<int8_t>() + d * plane;
+    ozaki_map(&maps.a[d], base, KS, nao, nsl, KS, nao * KS, bk, 128);
+    ozaki_map(&maps.b[d], base, KS, nao, nsl, KS, nao * KS, bk, kOzBN);
+  }
+  OzakiArgs a{};
+  a.M = (int)nao;
+  a.N = (int)nao;
+  a.ktiles = (int)(KS / bk);
+  a.ea = p.ws_oz_ex.as<int>();
+  a.ea_stride = nao;
+  a.eb = p.ws_oz_ex.as<int>();
+  a.eb_stride = nao;
+  a.b_batched = 1;
+  a.ld_out = nao;
+  a.batch_stride_out = nao * nao;
+  a.err = p.ws_oz_err.as<int>();
+  for (int64_t z0 = 0; z0 < nsl; z0 += 65535) {
+    const int64_t nz = std::min<int64_t>(65535, nsl - z0);
+    a.plane0 = (int)z0;
+    a.out = p.ws_oz_kp.as<double>() + z0 * nao * nao;
+    ozaki_launch(ND, maps, a, (int)nz, s);
+  }
+  const int64_t n = nao * nao;
+  reduce_slices_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p.ws_oz_kp.as<double>(), nsl, n,
+                                                                   sign, beta0 ? 1 : 0, K);
+  DFJK_LAUNCHED();
   check_oz_err(p, s);
 }
 

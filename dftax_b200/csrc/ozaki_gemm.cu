@@ -14,8 +14,8 @@
 //
 // Tiles: 128 (m) x 80 (n) x BK (k, bytes), K-major operands, TMA with the
 // BK-byte swizzle into an mbarrier ring (ND digit planes per operand per
-// stage). Two shapes are compiled: ND 4 with BK 128 (104 KB stages) and ND 6
-// with BK 64 (78 KB stages), both double-buffered. Warp 0 lane 0 issues
+// stage). Three shapes are compiled: ND 4 with BK 128 (104 KB stages), ND 5
+// and ND 6 with BK 64 (65 and 78 KB stages), all double-buffered. Warp 0 lane 0 issues
 // copies, warp 1 lane 0 issues MMAs (BK/32 per digit pair per k tile), all
 // four warps drain tensor memory (warp w owns rows 32w..32w+31). Every wait
 // is bounded (4 s of %globaltimer); a timeout sets *err, skips the remaining
@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n0 = blockIdx.x * kBN, m0 = blockIdx.y * kBM, z = blockIdx.z;
   const int nk = a.ktiles;
+  const int bz = a.b_batched ? a.plane0 + z : 0;   // B plane (and exponent set) of this CTA
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
 #pragma unroll
       for (int d = 0; d < ND; ++d) {
         tma_load_3d(smem_u32(st + d * A_TILE), &maps.a[d], full, i * BK, m0, a.plane0 + z);
-        tma_load_3d(smem_u32(st + ND * A_TILE + d * B_TILE), &maps.b[d], full, i * BK, n0, 0);
+        tma_load_3d(smem_u32(st + ND * A_TILE + d * B_TILE), &maps.b[d], full, i * BK, n0, bz);
       }
       ++issued;
     }
@@ -236,6 +237,7 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
     const int era = row < a.M ? a.ea[(int64_t)(a.plane0 + z) * a.ea_stride + row] : 0;
     double* orow = a.out + (int64_t)z * a.batch_stride_out + (int64_t)row * a.ld_out;
+    const int* ebz = a.eb + (int64_t)bz * a.eb_stride;
     for (int c = 0; c < kBN; c += 16) {
       int v[ND][16];
 #pragma unroll
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
         double t = 0.0;
 #pragma unroll
         for (int o = ND - 1; o >= 0; --o) t = t * 0x1p-7 + (double)v[o][j];
-        orow[col] = ldexp(t, era + a.eb[col] - 14);
+        orow[col] = ldexp(t, era + ebz[col] - 14);
       }
     }
   }
@@ -298,7 +300,7 @@ void launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t 
 
 }  // namespace
 
-int ozaki_box_k(int ndig) { return ndig == 6 ? 64 : 128; }
+int ozaki_box_k(int ndig) { return ndig == 4 ? 128 : 64; }
 
 void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
                int64_t stride1, int64_t stride2, int box_k, int box1) {
@@ -319,6 +321,7 @@ void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t
 void ozaki_launch(int ndig, const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
   if (grid_z <= 0 || a.M <= 0 || a.N <= 0) return;
   if (ndig == 4) launch<4, 128>(maps, a, grid_z, s);
+  else if (ndig == 5) launch<5, 64>(maps, a, grid_z, s);
   else if (ndig == 6) launch<6, 64>(maps, a, grid_z, s);
   else fail(DFJK_ERR_INVALID, "unsupported digit count %d", ndig);
 }
