@@ -26,7 +26,7 @@ EXPORTS = (
     "dfjk_plan_create", "dfjk_plan_destroy", "dfjk_plan_get_info", "dfjk_build", "dfjk_jk",
     "dfjk_jk_host", "dfjk_energy", "dfjk_eri3c_dense", "dfjk_eri2c_dense", "dfjk_metric_pinv",
     "dfjk_kept_pairs", "dfjk_boys", "dfjk_phase_times", "dfjk_kernel_launches",
-    "dfjk_j_noalloc",
+    "dfjk_j_noalloc", "dfjk_trim",
 )
 PHASES = ("metric", "pairs", "eri3c", "bgemm", "j", "khalf", "ksyrk", "kplanes")
 
@@ -98,6 +98,7 @@ def load(path: str | None = None):
         "dfjk_phase_times": (c_int, [V, P(c_double), c_int32]),
         "dfjk_kernel_launches": (c_int64, []),
         "dfjk_j_noalloc": (c_int, [V, V, V, c_int64, V, V]),
+        "dfjk_trim": (c_int, [V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -67,6 +67,10 @@ class Context:
     def last_error(self) -> str:
         return self.lib.dfjk_last_error(self.h).decode()
 
+    def trim(self):
+        """Return the device memory cached from destroyed plans to the driver."""
+        check(self.lib.dfjk_trim(self.h), self.h)
+
     def boys(self, t, nmax: int):
         """F_0..F_nmax at the points t (host array in, host array out)."""
         torch = _torch()

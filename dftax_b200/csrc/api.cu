@@ -1,13 +1,16 @@
 // Host side of the dfjk library: context, plan (shells, screening, layouts),
 // build (metric factor, 3-center rows, B) and the C ABI entry points.
 #include "internal.h"
+#include "ozaki.h"
 
 #include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+#include <thread>
 
 namespace dfjk {
 
@@ -20,16 +23,105 @@ void fail(dfjk_status code, const char* fmt, ...) {
   throw Error{code, buf};
 }
 
+// ---------------------------------------------------------------------------
+// Device memory cache. Plans are made one after another (one per geometry,
+// one per request of a serving loop) with buffers of the same sizes, and
+// cudaMalloc of tens of GB plus cudaFree (which synchronizes the device) cost
+// ~100 ms per (H2O)_32 plan. Freed buffers are kept per device and handed out
+// again to requests of at most their size and at least 3/4 of it. A cached
+// buffer may still be read by work queued before it was freed, so reusing it
+// first synchronizes the device, unless the device was synchronized after the
+// buffer was freed (epoch). A failed cudaMalloc empties the cache and retries;
+// dfjk_trim empties it on request.
+// ---------------------------------------------------------------------------
+
+namespace {
+struct Cached {
+  void* p;
+  size_t bytes;
+  uint64_t epoch;
+};
+std::mutex g_cache_mu;
+// never destroyed: cudaFree at process exit could run after the driver shut down
+std::vector<std::vector<Cached>>& cache() {
+  static auto* c = new std::vector<std::vector<Cached>>(64);
+  return *c;
+}
+std::vector<uint64_t>& epochs() {
+  static auto* e = new std::vector<uint64_t>(64, 0);
+  return *e;
+}
+
+void* cache_take(int dev, size_t n, size_t* got) {
+  bool need_sync = false;
+  void* p = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto& v = cache()[dev];
+    size_t best = v.size();
+    for (size_t i = 0; i < v.size(); ++i)
+      if (v[i].bytes >= n && n >= v[i].bytes / 4 * 3 &&
+          (best == v.size() || v[i].bytes < v[best].bytes))
+        best = i;
+    if (best == v.size()) return nullptr;
+    p = v[best].p;
+    *got = v[best].bytes;
+    need_sync = v[best].epoch == epochs()[dev];
+    v.erase(v.begin() + best);
+  }
+  if (need_sync) {
+    DFJK_CUDA(cudaDeviceSynchronize());
+    device_synchronized(dev);
+  }
+  return p;
+}
+}  // namespace
+
+void device_synchronized(int dev) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  if (dev >= 0 && dev < (int)epochs().size()) epochs()[dev]++;
+}
+
+void cache_trim(int dev) {
+  std::vector<Cached> v;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (dev < 0 || dev >= (int)cache().size()) return;
+    v.swap(cache()[dev]);
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(dev);
+  for (auto& c : v) cudaFree(c.p);
+  cudaSetDevice(cur);
+}
+
 void DevBuf::alloc(size_t n) {
   free();
   if (n == 0) n = 16;
+  int d = 0;
+  DFJK_CUDA(cudaGetDevice(&d));
+  if (d >= (int)cache().size()) fail(DFJK_ERR_INVALID, "device ordinal %d out of range", d);
+  size_t got = 0;
+  if (void* c = cache_take(d, n, &got)) {
+    p = c;
+    bytes = got;
+    dev = d;
+    return;
+  }
   cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cache_trim(d);
+    e = cudaMalloc(&p, n);
+  }
   if (e != cudaSuccess) {
     p = nullptr;
     cudaGetLastError();
     fail(DFJK_ERR_MEMORY, "cudaMalloc of %zu bytes failed: %s", n, cudaGetErrorString(e));
   }
   bytes = n;
+  dev = d;
 }
 
 static std::atomic<int64_t> g_launches{0};
@@ -64,7 +156,10 @@ void PhaseTimer::destroy() {
 }
 
 void DevBuf::free() {
-  if (p) cudaFree(p);
+  if (p) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    cache()[dev].push_back({p, bytes, epochs()[dev]});
+  }
   p = nullptr;
   bytes = 0;
 }
@@ -240,12 +335,39 @@ static void parse_basis(const dfjk_basis* b, const char* what, int lmax_supporte
       fail(DFJK_ERR_INVALID, "%s basis: cart2sph has %d columns, shells need %d", what, b->nsph, sh.nout);
     const double* C = b->cart2sph;
     const int ns = b->nsph;
+    // sum |C| over each shell's rows, read by several host threads (the
+    // auxiliary matrix is hundreds of MB); four partial sums per row
+    std::vector<double> row_abs(sh.n, 0.0);
+    auto scan = [&](int sa, int sb) {
+      for (int s = sa; s < sb; ++s) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = 0; i < ncart(sh.l[s]); ++i) {
+          const double* r = C + (int64_t)(sh.row0[s] + i) * ns;
+          int j = 0;
+          for (; j + 4 <= ns; j += 4)
+            for (int u = 0; u < 4; ++u) acc[u] += std::fabs(r[j + u]);
+          for (; j < ns; ++j) acc[0] += std::fabs(r[j]);
+        }
+        row_abs[s] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+      }
+    };
+    const int64_t cells = (int64_t)sh.ncart * ns;
+    const int nth = cells > (1 << 22)
+                        ? (int)std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()))
+                        : 1;
+    {
+      std::vector<std::thread> th;
+      for (int t = 1; t < nth; ++t)
+        th.emplace_back(scan, (int)((int64_t)sh.n * t / nth), (int)((int64_t)sh.n * (t + 1) / nth));
+      scan(0, sh.n / nth);
+      for (auto& x : th) x.join();
+    }
     for (int s = 0; s < sh.n; ++s) {
       const int l = sh.l[s], nc = ncart(l), no = 2 * l + 1, r0 = sh.row0[s], c0 = sh.out0[s];
-      double rows = 0.0, inb = 0.0;
+      const double rows = row_abs[s];
+      double inb = 0.0;
       std::vector<double> blkv((size_t)nc * no);
       for (int i = 0; i < nc; ++i) {
-        for (int j = 0; j < ns; ++j) rows += std::fabs(C[(int64_t)(r0 + i) * ns + j]);
         for (int j = 0; j < no; ++j) {
           const double v = C[(int64_t)(r0 + i) * ns + c0 + j];
           blkv[i * no + j] = v;
@@ -538,6 +660,10 @@ void build(Plan& p, cudaStream_t s) {
   p.built = 0;
   for (int ph = kPhMetric; ph <= kPhBgemm; ++ph) p.timer.reset(ph);
   p.timer.reset(kPhKplanes);
+  // The eigensolver keeps the whole device busy: running the 3-center rows
+  // beside it on a second stream (at either priority) was measured to save
+  // under 3% of a (H2O)_32 build while holding the whole tensor, so the
+  // phases run in order on s.
   p.timer.mark(kPhMetric, s);
   compute_metric_factor(p, s);
   p.timer.mark(kPhMetric, s);
@@ -545,16 +671,21 @@ void build(Plan& p, cudaStream_t s) {
   launch_pair_setup(p, s);
   p.timer.mark(kPhPairs, s);
   p.d_B.ensure((size_t)std::max<int64_t>(p.nrows, 1) * p.ldb * sizeof(double));
+  const bool mixed = p.opts.precision == DFJK_MIXED;
   const int64_t ld = p.naux;
+  const int64_t kp = (p.naux + 15) / 16 * 16;
   auto chunks = pair_chunks(p, ld, chunk_budget(p));
   int64_t maxrows = 1;
   for (auto& ch : chunks) maxrows = std::max(maxrows, rows_of(p, ch.first, ch.second));
   DevBuf& raw = p.ws_raw;
   raw.ensure((size_t)maxrows * ld * sizeof(double));
+  if (mixed) {
+    ozaki_prepare_l(p, s);
+    p.ws_oz_raw.ensure((size_t)kOzBDigits * maxrows * kp);
+    p.ws_oz_er.ensure((size_t)maxrows * sizeof(int));
+  }
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
   const double one = 1.0, zero = 0.0;
-  const bool mixed = p.opts.precision == DFJK_MIXED;
-  if (mixed) ozaki_prepare_l(p, s);
   for (auto& ch : chunks) {
     const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
     p.timer.mark(kPhEri3c, s);
@@ -563,7 +694,10 @@ void build(Plan& p, cudaStream_t s) {
     // B[r0:r0+nr, :] = raw (nr x naux) . L (naux x ldb)
     p.timer.mark(kPhBgemm, s);
     if (mixed) {
-      ozaki_bgemm(p, raw.as<double>(), nr, p.d_B.as<double>() + r0 * p.ldb, s);
+      ozaki_split_raw(p, raw.as<double>(), nr, p.ws_oz_raw.as<int8_t>(), nr * kp,
+                      p.ws_oz_er.as<int>(), s);
+      ozaki_bgemm(p, p.ws_oz_raw.as<int8_t>(), nr * kp, p.ws_oz_er.as<int>(), nr,
+                  p.d_B.as<double>() + r0 * p.ldb, s);
     } else {
       // column-major view: B^T = L^T raw^T
       DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)p.ldb, (int)nr, (int)p.naux,
@@ -732,7 +866,10 @@ dfjk_status dfjk_destroy(dfjk_ctx* h) {
   cudaSetDevice(h->c.device);
   if (h->c.cublas) cublasDestroy(h->c.cublas);
   if (h->c.cusolver) cusolverDnDestroy(h->c.cusolver);
+  const int dev = h->c.device;
+  cudaDeviceSynchronize();
   delete h;
+  dfjk::cache_trim(dev);
   return DFJK_OK;
 }
 
@@ -765,8 +902,20 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
 
 dfjk_status dfjk_plan_destroy(dfjk_plan* pl) {
   if (!pl) return DFJK_OK;
-  cudaSetDevice(pl->p.ctx->device);
+  const int dev = pl->p.ctx->device;
+  cudaSetDevice(dev);
+  // work queued on the plan's buffers ends here; they go back to the cache idle
+  cudaDeviceSynchronize();
   delete pl;
+  dfjk::device_synchronized(dev);
+  return DFJK_OK;
+}
+
+dfjk_status dfjk_trim(dfjk_ctx* h) {
+  if (!h) return DFJK_ERR_INVALID;
+  cudaSetDevice(h->c.device);
+  cudaDeviceSynchronize();
+  dfjk::cache_trim(h->c.device);
   return DFJK_OK;
 }
 

@@ -66,10 +66,15 @@ struct Error {
     ::dfjk::count_launch();             \
   } while (0)
 
-// Device buffer owned by a plan or context.
+// Device memory cache (api.cu): freed DevBufs are kept for reuse per device.
+void device_synchronized(int dev);   // after a cudaDeviceSynchronize on dev
+void cache_trim(int dev);            // cudaFree every cached buffer of dev
+
+// Device buffer owned by a plan or context (allocated through the cache).
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  int dev = 0;
   void alloc(size_t n);
   void free();
   // grow-only: keep the allocation when it is already large enough
@@ -211,7 +216,10 @@ struct Plan {
 
 // ---- mixed precision on the int8 tensor cores (ozaki.cu) ----
 void ozaki_prepare_l(Plan& p, cudaStream_t s);
-void ozaki_bgemm(Plan& p, const double* raw, int64_t nr, double* Bout, cudaStream_t s);
+void ozaki_split_raw(Plan& p, const double* raw, int64_t nr, int8_t* planes, int64_t plane_stride,
+                     int* e, cudaStream_t s);
+void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int* e, int64_t nr,
+                 double* Bout, cudaStream_t s);
 void build_ozaki_planes(Plan& p, cudaStream_t s);
 void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s);
 void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStream_t s);

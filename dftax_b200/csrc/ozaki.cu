@@ -300,18 +300,25 @@ void ozaki_prepare_l(Plan& p, cudaStream_t s) {
   DFJK_CUDA(cudaMemsetAsync(p.ws_oz_err.p, 0, sizeof(int), s));
 }
 
-// Bout[r][x] (ld ldb) = sum_P raw[r][P] L[P][x] for nr rows of raw (ld naux)
-void ozaki_bgemm(Plan& p, const double* raw, int64_t nr, double* Bout, cudaStream_t s) {
+// Digit planes of nr raw 3-center rows (ld naux): planes[d * plane_stride +
+// row * naux_p16 + k], row exponents e[row]
+void ozaki_split_raw(Plan& p, const double* raw, int64_t nr, int8_t* planes, int64_t plane_stride,
+                     int* e, cudaStream_t s) {
+  if (nr <= 0) return;
+  p.naux_p16 = (p.naux + 15) / 16 * 16;
+  split_rows_kernel<kOzBDigits><<<(unsigned)nr, 256, 0, s>>>(raw, p.naux, p.naux, p.naux_p16, e,
+                                                             plane_stride, planes);
+  DFJK_LAUNCHED();
+}
+
+// Bout[r][x] (ld ldb) = sum_P raw[r][P] L[P][x] for nr rows given as digit
+// planes (layout of ozaki_split_raw) and their row exponents
+void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int* e, int64_t nr,
+                 double* Bout, cudaStream_t s) {
   if (nr <= 0) return;
   constexpr int ND = kOzBDigits;
   const int bk = ozaki_box_k(ND);
   const int64_t kp = p.naux_p16;
-  const int64_t plane = nr * kp;
-  p.ws_oz_raw.ensure((size_t)ND * plane);
-  p.ws_oz_er.ensure((size_t)nr * sizeof(int));
-  split_rows_kernel<ND><<<(unsigned)nr, 256, 0, s>>>(raw, p.naux, p.naux, kp, p.ws_oz_er.as<int>(),
-                                                     plane, p.ws_oz_raw.as<int8_t>());
-  DFJK_LAUNCHED();
   OzakiMaps maps;
   const int64_t lplane = p.ldb * kp;
   for (int d = 0; d < ND; ++d)
@@ -331,10 +338,10 @@ void ozaki_bgemm(Plan& p, const double* raw, int64_t nr, double* Bout, cudaStrea
   for (int64_t m0 = 0; m0 < nr; m0 += step) {
     const int64_t mr = std::min(step, nr - m0);
     for (int d = 0; d < ND; ++d)
-      ozaki_map(&maps.a[d], p.ws_oz_raw.as<int8_t>() + d * plane + m0 * kp, p.naux, mr, 1, kp, plane,
+      ozaki_map(&maps.a[d], planes + d * plane_stride + m0 * kp, p.naux, mr, 1, kp, plane_stride,
                 bk, 128);
     a.M = (int)mr;
-    a.ea = p.ws_oz_er.as<int>() + m0;
+    a.ea = e + m0;
     a.out = Bout + m0 * p.ldb;
     ozaki_launch(ND, maps, a, 1, s);
   }

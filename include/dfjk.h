@@ -85,8 +85,16 @@ void dfjk_default_options(dfjk_options* opts);
 
 /* Context: device, library handles and the Boys table (dftax/energy/boys.py:81-123). */
 dfjk_status dfjk_create(int device, dfjk_ctx** ctx);
+/* Also releases the device memory cached on the context's device (dfjk_trim). */
 dfjk_status dfjk_destroy(dfjk_ctx* ctx);
 const char* dfjk_last_error(const dfjk_ctx* ctx);
+
+/* Device memory of destroyed plans is kept by the library, per device, and
+ * handed to the next plans (plans of one system, made one after another, get
+ * their buffers back without cudaMalloc/cudaFree). dfjk_trim synchronizes the
+ * context's device and returns that cached memory to the driver; a failed
+ * allocation does the same before it retries. No counterpart in the reference. */
+dfjk_status dfjk_trim(dfjk_ctx* ctx);
 
 /* Plan: shells, Schwarz-kept shell pairs, class buckets, device layout.
  * Replaces plan_eri3c / plan_pairs / _shell_pair_keep
