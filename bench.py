@@ -379,10 +379,13 @@ def run_ours(args, rank, world, local_rank):
                   "in-bench cuBLAS DGEMM 8192^3 burst", "nao (nao+1) nfit nocc"),
     }
     if mixed:
-        units["bgemm"] = ("tensor", 21 * 2.0 * nrows * naux * nfit / 1e12, "TOP/s", i8, i8_src,
-                          "int8 ops: 21 digit products x 2 nrows naux nfit")
+        # digit products per product: 5 digits -> 15, 4 digits -> 10
+        units["bgemm"] = ("tensor", 15 * 2.0 * nrows * naux * nfit / 1e12, "TOP/s", i8, i8_src,
+                          "int8 ops: 15 digit products x 2 nrows naux nfit")
         units["khalf"] = ("tensor", 10 * 2.0 * nfit * nao * nao * nocc / 1e12, "TOP/s", i8, i8_src,
                           "int8 ops: 10 digit products x 2 nfit nao^2 nocc")
+        units["ksyrk"] = ("tensor", 15 * 2.0 * nao * nao * nfit * nocc / 1e12, "TOP/s", i8, i8_src,
+                          "int8 ops: 15 digit products x 2 nao^2 nfit nocc (full square)")
         units["kplanes"] = ("hbm", (2 * 8.0 * (2 * nrows - nao) * nfit + 4.0 * nfit * nao * nao_p) / 1e9,
                             "GB/s", hbm, f"{src} hbm_gbs",
                             "B gathered twice per AO list + 4 int8 digit planes written")

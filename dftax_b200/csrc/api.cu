@@ -891,6 +891,11 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
     if (pl->p.opts.precision != DFJK_FP64 && pl->p.opts.precision != DFJK_MIXED)
       fail(DFJK_ERR_INVALID, "unknown precision %d", pl->p.opts.precision);
     make_plan(pl->p, orb, aux);
+    // the int8 products are exact for dot products of at most kOzMaxK terms
+    if (pl->p.opts.precision == DFJK_MIXED &&
+        (pl->p.naux > kOzMaxK || pl->p.nao > kOzMaxK))
+      fail(DFJK_ERR_UNSUPPORTED, "mixed precision supports nao, naux <= %lld (got %d, %d)",
+           (long long)kOzMaxK, pl->p.nao, pl->p.naux);
   });
   if (r != DFJK_OK) {
     delete pl;

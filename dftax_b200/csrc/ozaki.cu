@@ -3,9 +3,10 @@
 //   B[r][x] = sum_P (ij|P)[r][P] L[P][x]      (build, per raw row chunk)
 //   X[m][x][i] = sum_n B_x[m][n] C'[n][i]     (K half transform, per call)
 //   K[m][n] = sum_(x,i) X[m][x][i] X[n][x][i]  (K accumulation, per call)
-// Both operands of each product are split into signed 7-bit digits under a
-// per-row exponent; outputs are float64. The integrals, the metric, its
-// factor L, the stored B and J stay float64.
+// Both operands of each product are split into signed int8 digits (a 7-bit
+// leading digit, then balanced 8-bit digits) under a per-row exponent;
+// outputs are float64. The integrals, the metric, its factor L, the stored B
+// and J stay float64.
 //
 // Accuracy findings behind the digit counts (device runs on water clusters,
 // against the float64 path of the same plan):
@@ -15,17 +16,18 @@
 //     toward zero (relative -3e-6 with one 64-deep k tile per partial, -2.7e-4
 //     with long partials; E off by 76 uHa .. 5.9 mHa for (H2O)_32);
 //   * int8 digits with int32 accumulation are exact: what is left is the
-//     digit truncation, 2^(1-7D) of each row's largest value for D digits;
-//   * the half transform B_x C is well conditioned: 4 digits give K within
-//     6.5e-9 relative and E within 2.5e-10 Ha for (H2O)_32;
+//     digit truncation, 2^-(8D) of 2^e (at most 2^(2-8D) of the row maximum)
+//     for D digits;
+//   * the half transform B_x C is well conditioned: 4 digits keep K within
+//     1e-9 relative for (H2O)_32;
 //   * the build product (ij|P) L is not: the columns of L for small metric
 //     eigenvalues cancel the smooth part of each (ij|P) row, which amplifies
-//     the truncation by up to the metric's condition number. With 4 digits,
-//     E moved by 1.5e-5 Ha for (H2O)_8 and 1.0e-4 Ha for (H2O)_32, so the
-//     build uses 6 digits (2^-41), 2^14 times finer;
+//     the truncation by up to the metric's condition number. With four 7-bit
+//     digits (2^-29), E moved by 1.5e-5 Ha for (H2O)_8 and 1.0e-4 Ha for
+//     (H2O)_32; the build uses 5 digits (2^-40): 4e-8 Ha for (H2O)_32;
 //   * K = X X^T sums nfit * nocc products per element, with strong
-//     cancellation off the diagonal: with 4 digits K moved by 2.9e-7 relative
-//     and E by 3.1e-6 Ha for (H2O)_32, so it uses 5 digits (2^-34).
+//     cancellation off the diagonal: with four 7-bit digits E moved by 3.1e-6
+//     Ha for (H2O)_32, so it uses 5 digits (2^-40).
 #include "ozaki.h"
 
 #include <algorithm>
@@ -40,19 +42,33 @@ __device__ __forceinline__ int row_exponent(double vmax) {
   return vmax > 0.0 ? ilogb(vmax) + 2 : 0;
 }
 
-// ND signed 7-bit digits: v 2^-e = sum_s d_s 2^(-7(s+1)) + r, |r| <= 2^(-7ND-1).
-// Every step is exact in float64: scaling by 128, rounding to an integer
-// (|d_s| <= 64) and subtracting it (|t - d_s| <= 1/2).
+// ND signed digits of t = v 2^-e (|t| < 1/2): a 7-bit leading digit, then
+// balanced 8-bit digits,
+//   t = d_0 2^-7 + sum_(s>=1) d_s 2^-(7+8s) + r,   |r| <= 2^-(8 ND),
+// with |d_0| <= 65 and -128 <= d_s <= 127 after the carries (a digit of +128
+// becomes -128 and carries one into the digit above). Every step is exact in
+// float64: scaling by a power of two, rounding to an integer and subtracting
+// it (|t - d| <= 1/2).
 template <int ND>
 __device__ __forceinline__ void digits(double v, int e, int8_t* d) {
-  double t = ldexp(v, -e);
+  double t = ldexp(v, -e) * 128.0;
+  int q[ND];
+  q[0] = (int)rint(t);
+  t -= q[0];
 #pragma unroll
-  for (int s = 0; s < ND; ++s) {
-    t *= 128.0;
-    const double q = rint(t);
-    d[s] = (int8_t)q;
-    t -= q;
+  for (int s = 1; s < ND; ++s) {
+    t *= 256.0;
+    q[s] = (int)rint(t);
+    t -= q[s];
   }
+#pragma unroll
+  for (int s = ND - 1; s >= 1; --s)
+    if (q[s] > 127) {
+      q[s] -= 256;
+      q[s - 1] += 1;
+    }
+#pragma unroll
+  for (int s = 0; s < ND; ++s) d[s] = (int8_t)q[s];
 }
 
 // Digit planes of the square B_x: A[d][x][m][nao_p] (4 digits) with row
@@ -317,13 +333,14 @@ void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int*
                  double* Bout, cudaStream_t s) {
   if (nr <= 0) return;
   constexpr int ND = kOzBDigits;
-  const int bk = ozaki_box_k(ND);
+  const OzakiShapeInfo sh = ozaki_shape(kOzBuild);
+  const int bk = sh.box_k;
   const int64_t kp = p.naux_p16;
   OzakiMaps maps;
   const int64_t lplane = p.ldb * kp;
   for (int d = 0; d < ND; ++d)
     ozaki_map(&maps.b[d], p.ws_oz_l.as<int8_t>() + d * lplane, p.naux, p.ldb, 1, kp, lplane, bk,
-              kOzBN);
+              sh.bn);
   OzakiArgs a{};
   a.N = (int)p.ldb;
   a.ktiles = (int)((p.naux + bk - 1) / bk);
@@ -343,7 +360,7 @@ void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int*
     a.M = (int)mr;
     a.ea = e + m0;
     a.out = Bout + m0 * p.ldb;
-    ozaki_launch(ND, maps, a, 1, s);
+    ozaki_launch(kOzBuild, maps, a, 1, s);
   }
   check_oz_err(p, s);
 }
@@ -361,7 +378,8 @@ void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s) {
 // X[m][x - x0][i] (float64, ld n * nsel) for fitted directions [x0, x0 + n)
 void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStream_t s) {
   constexpr int ND = kOzKDigits;
-  const int bk = ozaki_box_k(ND);
+  const OzakiShapeInfo sh = ozaki_shape(kOzHalf);
+  const int bk = sh.box_k;
   const int64_t nao = p.nao, nao_p = p.nao_p16;
   const int64_t plane = p.nfit * nao * nao_p;
   OzakiMaps maps;
@@ -369,7 +387,7 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
     ozaki_map(&maps.a[d], p.d_oz_a.as<int8_t>() + d * plane, nao, nao, p.nfit, nao_p, nao * nao_p,
               bk, 128);
     ozaki_map(&maps.b[d], p.ws_oz_c.as<int8_t>() + d * nsel * nao_p, nao, nsel, 1, nao_p,
-              nsel * nao_p, bk, kOzBN);
+              nsel * nao_p, bk, sh.bn);
   }
   OzakiArgs a{};
   a.M = (int)nao;
@@ -386,7 +404,7 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
     const int64_t nz = std::min<int64_t>(65535, n - z0);
     a.plane0 = (int)(x0 + z0);
     a.out = X + z0 * nsel;
-    ozaki_launch(ND, maps, a, (int)nz, s);
+    ozaki_launch(kOzHalf, maps, a, (int)nz, s);
   }
   check_oz_err(p, s);
 }
@@ -399,7 +417,9 @@ void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, d
                 cudaStream_t s) {
   constexpr int ND = kOzSDigits;
   constexpr int64_t KS = kOzSlice;
-  const int bk = ozaki_box_k(ND);
+  static_assert(KS <= kOzMaxK, "a k slice must stay within the exact int32 range");
+  const OzakiShapeInfo sh = ozaki_shape(kOzSyrk);
+  const int bk = sh.box_k;
   const int64_t nao = p.nao;
   const int64_t nsl = (kt + KS - 1) / KS;
   const int64_t plane = nsl * nao * KS;
@@ -413,7 +433,7 @@ void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, d
   for (int d = 0; d < ND; ++d) {
     const int8_t* base = p.ws_oz_x.as<int8_t>() + d * plane;
     ozaki_map(&maps.a[d], base, KS, nao, nsl, KS, nao * KS, bk, 128);
-    ozaki_map(&maps.b[d], base, KS, nao, nsl, KS, nao * KS, bk, kOzBN);
+    ozaki_map(&maps.b[d], base, KS, nao, nsl, KS, nao * KS, bk, sh.bn);
   }
   OzakiArgs a{};
   a.M = (int)nao;
@@ -431,7 +451,7 @@ void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, d
     const int64_t nz = std::min<int64_t>(65535, nsl - z0);
     a.plane0 = (int)z0;
     a.out = p.ws_oz_kp.as<double>() + z0 * nao * nao;
-    ozaki_launch(ND, maps, a, (int)nz, s);
+    ozaki_launch(kOzSyrk, maps, a, (int)nz, s);
   }
   const int64_t n = nao * nao;
   reduce_slices_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p.ws_oz_kp.as<double>(), nsl, n,

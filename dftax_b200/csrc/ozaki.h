@@ -8,21 +8,29 @@
 
 namespace dfjk {
 
-constexpr int kOzBN = 80;          // n tile
-constexpr int kOzKDigits = 4;      // K half transform: 28 bits per value
-constexpr int kOzBDigits = 6;      // B = (ij|P) L: 42 bits per value (see ozaki.cu)
-constexpr int kOzSDigits = 5;      // K = X X^T: 35 bits per value
-constexpr int kOzMaxDigits = 6;
+constexpr int kOzKDigits = 4;      // K half transform: 2^-32 of each row's scale
+constexpr int kOzBDigits = 5;      // B = (ij|P) L: 2^-40 (see ozaki.cu)
+constexpr int kOzSDigits = 5;      // K = X X^T: 2^-40
+constexpr int kOzMaxDigits = 5;
+// longest exact dot product: 5 digits, order 4 sums 2*65*128 + 3*128*128 per k
+constexpr int64_t kOzMaxK = 32640;
 constexpr int64_t kOzSlice = 8192;  // k bytes per slice of the K = X X^T product
 
+// The products and the tile shape each one runs with (ozaki_gemm.cu).
+enum OzakiShape { kOzBuild = 0, kOzHalf = 1, kOzSyrk = 2 };
+struct OzakiShapeInfo {
+  int digits, box_k, bn, stages;   // digits per value, k tile bytes, n tile, ring depth
+};
+OzakiShapeInfo ozaki_shape(OzakiShape shape);
+
 struct OzakiMaps {
-  CUtensorMap a[kOzMaxDigits];   // A digit planes, box (k tile bytes, 128 rows, 1)
-  CUtensorMap b[kOzMaxDigits];   // B digit planes, box (k tile bytes, kOzBN rows, 1)
+  CUtensorMap a[kOzMaxDigits];   // A digit planes, box (box_k, 128 rows, 1)
+  CUtensorMap b[kOzMaxDigits];   // B digit planes, box (box_k, bn rows, 1)
 };
 
 struct OzakiArgs {
   int M, N;                // output extent (rows of A, rows of B)
-  int ktiles;              // k tiles of ozaki_box_k(ndig) bytes
+  int ktiles;              // k tiles of the shape's box_k bytes
   int plane0;              // A plane of blockIdx.z == 0
   const int* ea;           // exponent per A row: ea[(plane0 + z) * ea_stride + row]
   int64_t ea_stride;
@@ -34,16 +42,13 @@ struct OzakiArgs {
   int* err;                // set non-zero when a bounded wait gives up
 };
 
-// k tile (bytes) of the kernel that runs ndig digits per value: 128 (4 digits,
-// 128-byte swizzle) or 64 (5 and 6 digits, 64-byte swizzle)
-int ozaki_box_k(int ndig);
-
 // 3-D int8 tensor map over [d2][d1][d0] (d0 contiguous; strides in bytes),
 // box (box_k, box1, 1) with the swizzle that matches box_k
 void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
                int64_t stride1, int64_t stride2, int box_k, int box1);
 
-// grid (ceil(N/kOzBN), ceil(M/128), grid_z); ndig is 4, 5 or 6
-void ozaki_launch(int ndig, const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s);
+// grid (ceil(N/bn), ceil(M/128), grid_z)
+void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, int grid_z,
+                  cudaStream_t s);
 
 }  // namespace dfjk

@@ -1,21 +1,25 @@
 // Exact-accumulation int8 GEMM on the 5th-generation tensor cores.
 //
 //   D[m][n] = 2^(ea[m] + eb[n]) * sum_k a[m][k] b[n][k]
-// where every value is stored as ND signed 7-bit digits under its row's
-// exponent: a = 2^ea * sum_s d_s 2^(-7(s+1)), |d_s| <= 64 (Ozaki-style
-// splitting). The ND(ND+1)/2 digit products of combined order o = s + t < ND
-// are accumulated EXACTLY in int32 (kind::i8 MMA), one tensor-memory
-// accumulator per order; the epilogue combines them in float64 with weights
-// 2^(-7(o+2)). The only error is the truncation of the digit expansion
-// (2^(1-7ND) of the row maximum); unlike fp32 accumulation there is no
-// rounding drift with k. (Float32 accumulation of split-bf16 products was
+// where every value is stored as ND signed int8 digits under its row's
+// exponent (Ozaki-style splitting): a = 2^ea * (d_0 2^-7 + sum_(s>=1) d_s
+// 2^-(7+8s)), a 7-bit leading digit and balanced 8-bit digits after it. Digit
+// s times digit t weighs 2^-(14+8(s+t)), so the ND(ND+1)/2 products of
+// combined order o = s + t < ND are accumulated EXACTLY in int32 (kind::i8
+// MMA), one tensor-memory accumulator per order, and the epilogue combines
+// them in float64 with weights 2^-(14+8o). Exactness needs k * (sum over an
+// order of |d_s d_t|) < 2^31: k <= kOzMaxK. The only error is the truncation
+// of the digit expansion (2^-(8 ND) of 2^e, at most 2^(2-8ND) of the row
+// maximum); unlike fp32 accumulation there is no rounding drift with k. (Float32 accumulation of split-bf16 products was
 // measured to bias K toward zero by ~1e-6 per 24 MMAs, growing with the k
 // length; that path was dropped.)
 //
-// Tiles: 128 (m) x 80 (n) x BK (k, bytes), K-major operands, TMA with the
-// BK-byte swizzle into an mbarrier ring (ND digit planes per operand per
-// stage). Three shapes are compiled: ND 4 with BK 128 (104 KB stages), ND 5
-// and ND 6 with BK 64 (65 and 78 KB stages), all double-buffered. Warp 0 lane 0 issues
+// Tiles: 128 (m) x BN (n) x BK (k, bytes), K-major operands, TMA with the
+// BK-byte swizzle into an ST-stage mbarrier ring (ND digit planes per operand
+// per stage). Two shapes are compiled: ND 4, BK 128, BN 80, two 104 KB stages
+// (K half transform: n = occupied orbitals, 160 = 2 x 80 for (H2O)_32), and
+// ND 5, BK 64, BN 96, three 70 KB stages (build product and K = X X^T;
+// 5 x 96 of the 512 TMEM columns). Warp 0 lane 0 issues
 // copies, warp 1 lane 0 issues MMAs (BK/32 per digit pair per k tile), all
 // four warps drain tensor memory (warp w owns rows 32w..32w+31). Every wait
 // is bounded (4 s of %globaltimer); a timeout sets *err, skips the remaining
@@ -29,7 +33,7 @@ namespace dfjk {
 
 namespace {
 
-constexpr int kBM = 128, kBN = kOzBN, kStages = 2;
+constexpr int kBM = 128;
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kWaitNs = 4000000000ull;
 
@@ -131,36 +135,36 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v) {
   for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
 }
 
-template <int ND, int BK>
+template <int ND, int BK, int BN, int ST>
 __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ OzakiMaps maps,
                                                         OzakiArgs a) {
   constexpr uint32_t A_TILE = kBM * BK;
-  constexpr uint32_t B_TILE = kBN * BK;
+  constexpr uint32_t B_TILE = BN * BK;
   constexpr uint32_t STAGE = ND * (A_TILE + B_TILE);
   constexpr int KSTEPS = BK / 32;   // one kind::i8 MMA covers 32 bytes of k
-  // accumulator o at column o * ACC (128 when they fit, else packed at kBN)
-  constexpr uint32_t ACC = (ND * 128 <= (int)kTmemCols) ? 128 : kBN;
+  // accumulator o at column o * ACC (128 when they fit, else packed at BN)
+  constexpr uint32_t ACC = (ND * 128 <= (int)kTmemCols) ? 128 : BN;
   static_assert(ND * ACC <= kTmemCols, "order accumulators exceed tensor memory");
   static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles must keep 1 KB alignment");
   // S32 accumulator (c_format 2), signed int8 A and B (format 1), N>>3, M>>4
-  constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
+  constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                              ((uint32_t)(kBM >> 4) << 24);
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * STAGE);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + ST * STAGE);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * ST + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * kBN, m0 = blockIdx.y * kBM, z = blockIdx.z;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * kBM, z = blockIdx.z;
   const int nk = a.ktiles;
   const int bz = a.b_batched ? a.plane0 + z : 0;   // B plane (and exponent set) of this CTA
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < ST; ++s) {
       mbar_init(smem_u32(&bars[s]), 1);
-      mbar_init(smem_u32(&bars[kStages + s]), 1);
+      mbar_init(smem_u32(&bars[ST + s]), 1);
     }
-    mbar_init(smem_u32(&bars[2 * kStages]), 1);
+    mbar_init(smem_u32(&bars[2 * ST]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -180,8 +184,8 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
     int issued = 0;
     bool ok = true;
     for (int i = 0; i < nk && ok; ++i) {
-      const int s = i % kStages;
-      if (i >= kStages) ok = mbar_wait(smem_u32(&bars[kStages + s]), ((i / kStages) - 1) & 1, a.err, 1);
+      const int s = i % ST;
+      if (i >= ST) ok = mbar_wait(smem_u32(&bars[ST + s]), ((i / ST) - 1) & 1, a.err, 1);
       if (!ok) break;
       const uint32_t full = smem_u32(&bars[s]);
       mbar_expect_tx(full, STAGE);
@@ -194,17 +198,17 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
       ++issued;
     }
     if (!ok) {
-      for (int i = issued - kStages > 0 ? issued - kStages : 0; i < issued; ++i) {
+      for (int i = issued - ST > 0 ? issued - ST : 0; i < issued; ++i) {
         const uint64_t t0 = now_ns();
-        while (!mbar_try(smem_u32(&bars[i % kStages]), (i / kStages) & 1) && now_ns() - t0 < kWaitNs)
+        while (!mbar_try(smem_u32(&bars[i % ST]), (i / ST) & 1) && now_ns() - t0 < kWaitNs)
           __nanosleep(64);
       }
     }
   } else if (threadIdx.x == 32 && nk > 0) {
     bool ok = true;
     for (int i = 0; i < nk; ++i) {
-      const int s = i % kStages;
-      ok = mbar_wait(smem_u32(&bars[s]), (i / kStages) & 1, a.err, 2);
+      const int s = i % ST;
+      ok = mbar_wait(smem_u32(&bars[s]), (i / ST) & 1, a.err, 2);
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t base = smem_u32(smem + s * STAGE);
@@ -223,13 +227,27 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
                     (i > 0 || sa > 0 || k > 0) ? 1u : 0u);
         }
       }
-      umma_commit(smem_u32(&bars[kStages + s]));
+      umma_commit(smem_u32(&bars[ST + s]));
     }
-    if (ok) umma_commit(smem_u32(&bars[2 * kStages]));
+    // also after a failed wait: the done barrier then tracks the MMAs already
+    // issued, so tensor memory is not freed under them
+    umma_commit(smem_u32(&bars[2 * ST]));
   }
   __syncwarp();
 
-  bool have = nk > 0 && mbar_wait(smem_u32(&bars[2 * kStages]), 0, a.err, 3);
+  bool have = false;
+  if (nk > 0) {
+    // bounded by time only: the MMAs must be finished before TMEM is freed
+    const uint64_t t0 = now_ns();
+    while (!(have = mbar_try(smem_u32(&bars[2 * ST]), 0))) {
+      if (now_ns() - t0 > kWaitNs) {
+        atomicCAS(a.err, 0, 3);
+        break;
+      }
+      __nanosleep(64);
+    }
+    have = have && *reinterpret_cast<volatile int*>(a.err) == 0;
+  }
   have = __all_sync(0xffffffffu, have);   // tcgen05.ld is warp-collective
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (have) {
@@ -238,7 +256,7 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
     const int era = row < a.M ? a.ea[(int64_t)(a.plane0 + z) * a.ea_stride + row] : 0;
     double* orow = a.out + (int64_t)z * a.batch_stride_out + (int64_t)row * a.ld_out;
     const int* ebz = a.eb + (int64_t)bz * a.eb_stride;
-    for (int c = 0; c < kBN; c += 16) {
+    for (int c = 0; c < BN; c += 16) {
       int v[ND][16];
 #pragma unroll
       for (int o = 0; o < ND; ++o) tmem_ld16(trow + (uint32_t)o * ACC + c, v[o]);
@@ -247,10 +265,10 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
       for (int j = 0; j < 16; ++j) {
         const int col = n0 + c + j;
         if (col >= a.N) break;
-        // sum_o acc_o 2^(-7(o+2)), highest order first
+        // sum_o acc_o 2^-(14+8o), highest order first
         double t = 0.0;
 #pragma unroll
-        for (int o = ND - 1; o >= 0; --o) t = t * 0x1p-7 + (double)v[o][j];
+        for (int o = ND - 1; o >= 0; --o) t = t * 0x1p-8 + (double)v[o][j];
         orow[col] = ldexp(t, era + ebz[col] - 14);
       }
     }
@@ -282,25 +300,33 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-template <int ND, int BK>
+template <int ND, int BK, int BN, int ST>
 constexpr size_t smem_bytes() {
-  return (size_t)kStages * ND * (kBM * BK + kBN * BK) + 1024 + 256;
+  return (size_t)ST * ND * (kBM * BK + BN * BK) + 1024 + 256;
 }
 
-template <int ND, int BK>
+template <int ND, int BK, int BN, int ST>
 void launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
-  constexpr size_t smem = smem_bytes<ND, BK>();
+  constexpr size_t smem = smem_bytes<ND, BK, BN, ST>();
   static_assert(smem <= 232448, "stages exceed the shared memory of one CTA");
-  dim3 grid((a.N + kBN - 1) / kBN, (a.M + kBM - 1) / kBM, grid_z);
-  DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8<ND, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-  ozaki_gemm_i8<ND, BK><<<grid, 128, smem, s>>>(maps, a);
+  dim3 grid((a.N + BN - 1) / BN, (a.M + kBM - 1) / kBM, grid_z);
+  DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8<ND, BK, BN, ST>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ozaki_gemm_i8<ND, BK, BN, ST><<<grid, 128, smem, s>>>(maps, a);
   DFJK_LAUNCHED();
 }
 
 }  // namespace
 
-int ozaki_box_k(int ndig) { return ndig == 4 ? 128 : 64; }
+// digits, k tile bytes, n tile, stages of each product (see ozaki.h)
+OzakiShapeInfo ozaki_shape(OzakiShape shape) {
+  switch (shape) {
+    case kOzHalf: return {kOzKDigits, 128, 80, 2};
+    case kOzBuild: return {kOzBDigits, 64, 96, 3};
+    case kOzSyrk: return {kOzSDigits, 64, 96, 3};
+  }
+  fail(DFJK_ERR_INVALID, "unknown int8 GEMM shape %d", (int)shape);
+}
 
 void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
                int64_t stride1, int64_t stride2, int box_k, int box1) {
@@ -318,12 +344,17 @@ void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t
   if (r != CUDA_SUCCESS) fail(DFJK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
 
-void ozaki_launch(int ndig, const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
+void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, int grid_z,
+                  cudaStream_t s) {
   if (grid_z <= 0 || a.M <= 0 || a.N <= 0) return;
-  if (ndig == 4) launch<4, 128>(maps, a, grid_z, s);
-  else if (ndig == 5) launch<5, 64>(maps, a, grid_z, s);
-  else if (ndig == 6) launch<6, 64>(maps, a, grid_z, s);
-  else fail(DFJK_ERR_INVALID, "unsupported digit count %d", ndig);
+  static_assert(kOzKDigits == 4 && kOzBDigits == 5 && kOzSDigits == 5,
+                "the compiled shapes follow the digit counts");
+  switch (shape) {
+    case kOzHalf: launch<4, 128, 80, 2>(maps, a, grid_z, s); return;
+    case kOzBuild:
+    case kOzSyrk: launch<5, 64, 96, 3>(maps, a, grid_z, s); return;
+  }
+  fail(DFJK_ERR_INVALID, "unknown int8 GEMM shape %d", (int)shape);
 }
 
 }  // namespace dfjk

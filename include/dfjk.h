@@ -40,8 +40,8 @@ typedef enum {
 enum {
   DFJK_FP64 = 0,  /* float64 integrals, B, J and K                               */
   DFJK_MIXED = 1  /* float64 integrals, metric, stored B and J; the products
-                     B = (ij|P) L, X = B_x C and K = X X^T (6, 4 and 5 digits
-                     per value) on int8 tensor cores with exact int32
+                     B = (ij|P) L, X = B_x C and K = X X^T (5, 4 and 5 int8
+                     digits per value) on int8 tensor cores with exact int32
                      accumulation and float64 epilogues; extra 4*nfit*nao^2
                      bytes of device memory                                     */
 };
