@@ -75,9 +75,12 @@ __device__ __forceinline__ void digits(double v, int e, int8_t* d) {
 // exponents ea[x][m], for XB fitted directions and one AO m per block. Row m
 // of B_x is gathered through m's list of (row of B, n) entries (both
 // triangles, screened pairs absent); pass 1 takes the row maxima, pass 2
-// (re-reading the same rows, now in L2) writes the digits into shared memory,
-// which then goes out as 16-byte stores. Loads are issued kU at a time per
-// thread so that the gathers overlap.
+// (re-reading the same rows, now in L2) packs the four digits of each value
+// into one 32-bit word of a shared-memory row per direction, and the rows go
+// out as one 32-bit word of 4 consecutive n per digit plane (a 4 x 4 byte
+// transpose). Loads are issued kU at a time per thread so the gathers overlap.
+// (Holding the values in registers between the passes, with 1024-thread
+// blocks, was measured 1.5x slower: the per-block setup then dominates.)
 template <int XB>
 __global__ void __launch_bounds__(256) kplanes_kernel(const double* __restrict__ B, int64_t ldb,
                                                       const int* __restrict__ kptr,
@@ -88,9 +91,11 @@ __global__ void __launch_bounds__(256) kplanes_kernel(const double* __restrict__
                                                       int8_t* __restrict__ out) {
   constexpr int G = 256 / XB;   // list entries in flight per block
   constexpr int kU = 8;
-  extern __shared__ __align__(16) int8_t sd[];   // [4][XB][nao_p]
+  // [XB][W] words, W = nao_p + 4: rows stay 16-byte aligned and start 4 banks apart
+  extern __shared__ __align__(16) uint32_t sw[];
   __shared__ double red[G][XB];
   __shared__ int sh_e[XB];
+  const int64_t W = nao_p + 4;
   const int m = blockIdx.x;
   const int64_t x0 = (int64_t)blockIdx.y * XB;
   const int lx = threadIdx.x % XB, g = threadIdx.x / XB;
@@ -113,9 +118,9 @@ __global__ void __launch_bounds__(256) kplanes_kernel(const double* __restrict__
     for (; e < e1; e += G) mx = fmax(mx, fabs(B[(int64_t)krow[e] * ldb + x]));
   }
   red[g][lx] = mx;
-  // zero the staging planes (screened n and the padding stay zero)
-  const int64_t nvec = 4 * XB * nao_p / 16;
-  for (int64_t q = threadIdx.x; q < nvec; q += 256) reinterpret_cast<int4*>(sd)[q] = make_int4(0, 0, 0, 0);
+  // zero the staging rows (screened n and the padding stay zero)
+  const int64_t nvec = XB * W / 4;
+  for (int64_t q = threadIdx.x; q < nvec; q += 256) reinterpret_cast<uint4*>(sw)[q] = make_uint4(0, 0, 0, 0);
   __syncthreads();
   if (threadIdx.x < XB) {
     double v = 0.0;
@@ -126,7 +131,14 @@ __global__ void __launch_bounds__(256) kplanes_kernel(const double* __restrict__
   }
   __syncthreads();
   const int ex = sh_e[lx];
+  auto pack = [&](double v) {
+    int8_t d[4];
+    digits<4>(v, ex, d);
+    return (uint32_t)(uint8_t)d[0] | ((uint32_t)(uint8_t)d[1] << 8) | ((uint32_t)(uint8_t)d[2] << 16) |
+           ((uint32_t)(uint8_t)d[3] << 24);
+  };
   if (xin) {
+    uint32_t* row = sw + lx * W;
     int e = e0 + g;
     for (; e + (kU - 1) * G < e1; e += kU * G) {
       int r[kU], n[kU];
@@ -139,29 +151,25 @@ __global__ void __launch_bounds__(256) kplanes_kernel(const double* __restrict__
 #pragma unroll
       for (int u = 0; u < kU; ++u) v[u] = B[(int64_t)r[u] * ldb + x];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        int8_t d[4];
-        digits<4>(v[u], ex, d);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) sd[((int64_t)s * XB + lx) * nao_p + n[u]] = d[s];
-      }
+      for (int u = 0; u < kU; ++u) row[n[u]] = pack(v[u]);
     }
-    for (; e < e1; e += G) {
-      int8_t d[4];
-      digits<4>(B[(int64_t)krow[e] * ldb + x], ex, d);
-      const int n = kn[e];
-#pragma unroll
-      for (int s = 0; s < 4; ++s) sd[((int64_t)s * XB + lx) * nao_p + n] = d[s];
-    }
+    for (; e < e1; e += G) row[kn[e]] = pack(B[(int64_t)krow[e] * ldb + x]);
   }
   __syncthreads();
-  const int64_t vrow = nao_p / 16;   // int4 per (digit, x) row
-  for (int64_t q = threadIdx.x; q < nvec; q += 256) {
-    const int64_t srow = q / vrow, c = q % vrow;
-    const int s = (int)(srow / XB), j = (int)(srow % XB);
+  const int64_t nq = nao_p / 4;   // groups of 4 n per row
+  for (int64_t q = threadIdx.x; q < XB * nq; q += 256) {
+    const int j = (int)(q / nq);
+    const int64_t c = q % nq;
     if (x0 + j >= nfit) continue;
-    int8_t* dst = out + s * plane + ((x0 + j) * nao + m) * nao_p;
-    reinterpret_cast<int4*>(dst)[c] = reinterpret_cast<const int4*>(sd)[q];
+    const uint4 w = *reinterpret_cast<const uint4*>(sw + j * W + 4 * c);
+    // byte d of the 4 words -> word of plane d
+    const uint32_t lo01 = __byte_perm(w.x, w.y, 0x5140), hi01 = __byte_perm(w.x, w.y, 0x7362);
+    const uint32_t lo23 = __byte_perm(w.z, w.w, 0x5140), hi23 = __byte_perm(w.z, w.w, 0x7362);
+    const uint32_t dw[4] = {__byte_perm(lo01, lo23, 0x5410), __byte_perm(lo01, lo23, 0x7632),
+                            __byte_perm(hi01, hi23, 0x5410), __byte_perm(hi01, hi23, 0x7632)};
+    const int64_t o = ((x0 + j) * nao + m) * nao_p;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) reinterpret_cast<uint32_t*>(out + d * plane + o)[c] = dw[d];
   }
 }
 
@@ -274,7 +282,7 @@ void check_oz_err(Plan& p, cudaStream_t s) {
 
 template <int XB>
 static void launch_kplanes(Plan& p, int64_t plane, cudaStream_t s) {
-  const size_t smem = (size_t)4 * XB * p.nao_p16;
+  const size_t smem = (size_t)4 * XB * (p.nao_p16 + 4);
   DFJK_CUDA(cudaFuncSetAttribute(kplanes_kernel<XB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
   const int64_t nxb = (p.nfit + XB - 1) / XB;
@@ -296,9 +304,9 @@ void build_ozaki_planes(Plan& p, cudaStream_t s) {
   const int64_t plane = nfit * nao * p.nao_p16;
   p.d_oz_a.ensure((size_t)kOzKDigits * plane);
   p.d_oz_ea.ensure((size_t)nfit * nao * sizeof(int));
-  // 16 directions per block while the staging planes fit in 160 KB of shared memory
-  if ((size_t)4 * 16 * p.nao_p16 <= (size_t)160 << 10) launch_kplanes<16>(p, plane, s);
-  else if ((size_t)4 * 4 * p.nao_p16 <= (size_t)200 << 10) launch_kplanes<4>(p, plane, s);
+  // 16 directions per block while the staging rows fit in 160 KB of shared memory
+  if ((size_t)4 * 16 * (p.nao_p16 + 4) <= (size_t)160 << 10) launch_kplanes<16>(p, plane, s);
+  else if ((size_t)4 * 4 * (p.nao_p16 + 4) <= (size_t)200 << 10) launch_kplanes<4>(p, plane, s);
   else fail(DFJK_ERR_UNSUPPORTED, "mixed precision supports nao <= 12800");
 }
 
