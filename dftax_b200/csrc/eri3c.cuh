@@ -30,12 +30,62 @@ __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
   const double C0 = a.aux.cen[3 * kc], C1 = a.aux.cen[3 * kc + 1], C2 = a.aux.cen[3 * kc + 2];
   const int cp0 = a.aux.prim0[kc], cnp = a.aux.nprim[kc];
 
+  const int64_t pp0 = a.pair_pp0[pr];
+  const int npp = a.pair_npp[pr];
+  const int64_t row0 = a.pair_row0[pr] - a.row_base;
+  const int col = a.col_base + slot * NC;
+
+  if (npp == 1 && cnp == 1) {
+    // One primitive triple (uncontracted shells): every (i, m) is final as
+    // soon as it is formed, so it goes straight to the output and no
+    // accumulator array is kept (that array lives in local memory).
+    const double P0 = a.pp_P[3 * pp0], P1 = a.pp_P[3 * pp0 + 1], P2 = a.pp_P[3 * pp0 + 2];
+    const double g = a.pp_g[pp0];
+    const double* E = a.esph + (pp0 - a.esph_pp0) * (NAB * NH);
+    const double gc = a.aux.pexp[cp0], cc = a.aux.pcoef[cp0];
+    const double rho = g * gc / (g + gc);
+    const double X = P0 - C0, Y = P1 - C1, Z = P2 - C2;
+    double F[M + 1];
+    boys_eval<M>(rho * (X * X + Y * Y + Z * Z), a.boys, a.boys_asym, F);
+    double R[NR];
+    hermite_r<M>(rho, X, Y, Z, F, R);
+    double hob = 1.0;
+    const double i2gc = -0.5 / gc;
+#pragma unroll
+    for (int k = 0; k < LC; ++k) hob *= i2gc;
+    const double pref = a.pp_pref[pp0] * cc * kTwoPi25 / (g * gc * sqrt(g + gc)) * hob;
+#pragma unroll 1
+    for (int m = 0; m < NC; ++m) {
+      double w[NH];
+#pragma unroll
+      for (int t = 0; t <= LAB; ++t)
+#pragma unroll
+        for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll
+          for (int v = 0; v <= LAB - t - u; ++v) {
+            double s = 0.0;
+#pragma unroll
+            for (int c = 0; c < NCC; ++c)
+              s += sT[c * NC + m] * R[hidx(t + comp_x(LC, c), u + comp_y(LC, c), v + comp_z(LC, c))];
+            w[hidx(t, u, v)] = s * pref;
+          }
+#pragma unroll 1
+      for (int i = 0; i < NAB; ++i) {
+        const double* Ei = E + i * NH;
+        double s = 0.0;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) s += __ldg(Ei + h) * w[h];
+        const int64_t o = (row0 + i) * a.ld + col + m;
+        if (a.out_f32) static_cast<float*>(a.out)[o] = (float)s;
+        else static_cast<double*>(a.out)[o] = s;
+      }
+    }
+    return;
+  }
+
   double acc[NAB * NC];
 #pragma unroll 1
   for (int q = 0; q < NAB * NC; ++q) acc[q] = 0.0;
-
-  const int64_t pp0 = a.pair_pp0[pr];
-  const int npp = a.pair_npp[pr];
 #pragma unroll 1
   for (int q = 0; q < npp; ++q) {
     const int64_t pp = pp0 + q;
@@ -84,8 +134,6 @@ __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
       }
     }
   }
-  const int64_t row0 = a.pair_row0[pr] - a.row_base;
-  const int col = a.col_base + slot * NC;
   if (a.out_f32) {
     float* out = static_cast<float*>(a.out);
 #pragma unroll 1
