@@ -163,62 +163,96 @@ static void j_from_gamma(Plan& p, const double* gamma, double* J, cudaStream_t s
 // K: half transform X[m][x][i] = sum_{(r, n) in list(m)} B[r][x0 + x] C'[n][i]
 // ---------------------------------------------------------------------------
 
-constexpr int kHtX = 64, kHtI = 64, kHtK = 16;
+// Block tile 64 (x) x 80 (i), 16 list entries per k chunk, on the float64
+// tensor cores (mma.sync m8n8k4 f64: tcgen05 has no float64 kind). Eight
+// warps as 4 (x, 16 rows) x 2 (i, 40 columns); a warp holds 2 x 5 fragments
+// of 8 x 8. Shared rows are padded to 68 / 84 doubles so that the fragment
+// loads (k = lane % 4, row = lane / 4) fall in distinct banks.
+constexpr int kHtX = 64, kHtI = 80, kHtK = 16, kHtPX = 68, kHtPI = 84;
+
+__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  // src-size 0 fills the 8 shared bytes with zeros (gmem must still be a valid address)
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
+                   static_cast<unsigned>(__cvta_generic_to_shared(smem))),
+               "l"(gmem), "r"(valid ? 8 : 0)
+               : "memory");
+}
 
 __global__ void __launch_bounds__(256) half_transform_kernel(
     const double* __restrict__ B, int64_t ldb, int64_t x0, int64_t xc, const double* __restrict__ Cp,
     int64_t ncol, const int* __restrict__ kptr, const int* __restrict__ krow,
     const int* __restrict__ kn, double* __restrict__ X) {
-  __shared__ double Bs[kHtK][kHtX];
-  __shared__ double Cs[kHtK][kHtI];
+  // two buffers: chunk c + 1 is copied (cp.async) while chunk c is multiplied
+  __shared__ double Bs[2][kHtK][kHtPX];
+  __shared__ double Cs[2][kHtK][kHtPI];
   const int m = blockIdx.x;
   const int64_t xt = (int64_t)blockIdx.y * kHtX;   // within the chunk
   const int64_t it = (int64_t)blockIdx.z * kHtI;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wx = (warp & 3) * 16, wi = (warp >> 2) * 40;
+  const int fr = lane >> 2, fk = lane & 3;   // fragment row / k of this lane
+  double acc[2][5][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 5; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
   const int e0 = kptr[m], e1 = kptr[m + 1];
-  for (int e = e0; e < e1; e += kHtK) {
-    // stage kHtK list entries: rows of B (x tile) and rows of C' (i tile)
+  // kHtK list entries: rows of B (x tile) and rows of C' (i tile)
+  auto stage = [&](int buf, int e) {
     for (int q = threadIdx.x; q < kHtK * kHtX; q += 256) {
       const int k = q / kHtX, x = q % kHtX;
-      double v = 0.0;
-      if (e + k < e1 && xt + x < xc) v = B[(int64_t)krow[e + k] * ldb + x0 + xt + x];
-      Bs[k][x] = v;
+      const bool ok = e + k < e1 && xt + x < xc;
+      cp_async8(&Bs[buf][k][x], ok ? B + (int64_t)krow[e + k] * ldb + x0 + xt + x : B, ok);
     }
     for (int q = threadIdx.x; q < kHtK * kHtI; q += 256) {
       const int k = q / kHtI, i = q % kHtI;
-      double v = 0.0;
-      if (e + k < e1 && it + i < ncol) v = Cp[(int64_t)kn[e + k] * ncol + it + i];
-      Cs[k][i] = v;
+      const bool ok = e + k < e1 && it + i < ncol;
+      cp_async8(&Cs[buf][k][i], ok ? Cp + (int64_t)kn[e + k] * ncol + it + i : Cp, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if (e0 < e1) stage(0, e0);
+  int buf = 0;
+  for (int e = e0; e < e1; e += kHtK, buf ^= 1) {
+    if (e + kHtK < e1) {
+      stage(buf ^ 1, e + kHtK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kHtK; ++k) {
-      double bx[4], ci[4];
+    for (int kk = 0; kk < kHtK; kk += 4) {
+      double af[2], bf[5];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) bx[a] = Bs[k][tx + 16 * a];
+      for (int a = 0; a < 2; ++a) af[a] = Bs[buf][kk + fk][wx + 8 * a + fr];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) ci[b] = Cs[k][ty + 16 * b];
+      for (int b = 0; b < 5; ++b) bf[b] = Cs[buf][kk + fk][wi + 8 * b + fr];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] += bx[a] * ci[b];
+        for (int b = 0; b < 5; ++b) dmma_8x8x4(acc[a][b], af[a], bf[b]);
     }
     __syncthreads();
   }
+  // accumulator (a, b, r) holds x = wx + 8a + lane / 4, i = wi + 8b + 2 (lane % 4) + r
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int64_t x = xt + tx + 16 * a;
+  for (int a = 0; a < 2; ++a) {
+    const int64_t x = xt + wx + 8 * a + fr;
     if (x >= xc) continue;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int64_t i = it + ty + 16 * b;
-      if (i < ncol) X[((int64_t)m * xc + x) * ncol + i] = acc[a][b];
-    }
+    for (int b = 0; b < 5; ++b)
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int64_t i = it + wi + 8 * b + 2 * fk + r;
+        if (i < ncol) X[((int64_t)m * xc + x) * ncol + i] = acc[a][b][r];
+      }
   }
 }
 
