@@ -212,6 +212,8 @@ struct Plan {
   DevBuf ws_oz_l, ws_oz_el, ws_oz_raw, ws_oz_er;
   // mixed precision: digit slices of X, their exponents and per-slice K partials
   DevBuf ws_oz_x, ws_oz_ex, ws_oz_kp;
+  // float64 K = X X^T: lower tile pairs and per-slice partials
+  DevBuf ws_syrk_tiles, ws_syrk;
 };
 
 // ---- mixed precision on the int8 tensor cores (ozaki.cu) ----

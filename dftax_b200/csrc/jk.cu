@@ -256,6 +256,92 @@ __global__ void __launch_bounds__(256) half_transform_kernel(
   }
 }
 
+// K partials on the float64 tensor cores: for the lower-triangle tile pair
+// (tm >= tn, 64 x 64) of blockIdx.x and the k slice blockIdx.y,
+// part[slice][tm*64 + r][tn*64 + c] = sum_k X[tm*64 + r][k] X[tn*64 + c][k]
+// over the slice (X row-major, nao x kt). Same fragment layout and cp.async
+// double buffering as the half transform; rows are staged k-major.
+constexpr int kSyT = 64, kSyK = 16, kSyP = 68;
+
+__global__ void __launch_bounds__(256) syrk_part_kernel(const double* __restrict__ X, int64_t nao,
+                                                        int64_t kt, int64_t kslice,
+                                                        const int2* __restrict__ tiles,
+                                                        double* __restrict__ part) {
+  __shared__ double As[2][kSyK][kSyP];
+  __shared__ double Bs[2][kSyK][kSyP];
+  const int2 tp = tiles[blockIdx.x];
+  const int64_t r0 = (int64_t)tp.x * kSyT, c0 = (int64_t)tp.y * kSyT;
+  const int64_t k0 = (int64_t)blockIdx.y * kslice;
+  const int64_t k1 = k0 + kslice < kt ? k0 + kslice : kt;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = (warp & 3) * 16, wc = (warp >> 2) * 32;
+  const int fr = lane >> 2, fk = lane & 3;
+  double acc[2][4][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  auto stage = [&](int buf, int64_t k) {
+    for (int q = threadIdx.x; q < kSyT * kSyK; q += 256) {
+      const int r = q / kSyK, kk = q % kSyK;
+      const bool ka = k + kk < k1;
+      const bool oa = ka && r0 + r < nao, ob = ka && c0 + r < nao;
+      cp_async8(&As[buf][kk][r], oa ? X + (r0 + r) * kt + k + kk : X, oa);
+      cp_async8(&Bs[buf][kk][r], ob ? X + (c0 + r) * kt + k + kk : X, ob);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if (k0 < k1) stage(0, k0);
+  int buf = 0;
+  for (int64_t k = k0; k < k1; k += kSyK, buf ^= 1) {
+    if (k + kSyK < k1) {
+      stage(buf ^ 1, k + kSyK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kSyK; kk += 4) {
+      double af[2], bf[4];
+#pragma unroll
+      for (int a = 0; a < 2; ++a) af[a] = As[buf][kk + fk][wr + 8 * a + fr];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bf[b] = Bs[buf][kk + fk][wc + 8 * b + fr];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b], af[a], bf[b]);
+    }
+    __syncthreads();
+  }
+  double* out = part + (int64_t)blockIdx.y * nao * nao;
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const int64_t r = r0 + wr + 8 * a + fr;
+    if (r >= nao) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int64_t c = c0 + wc + 8 * b + 2 * fk + q;
+        if (c < nao) out[r * nao + c] = acc[a][b][q];
+      }
+  }
+}
+
+// K[i][j] = (beta0 ? 0 : K[i][j]) + sign * sum_s part[s][max(i,j)][min(i,j)], s in order
+__global__ void syrk_reduce_kernel(const double* __restrict__ part, int64_t nsplit, int64_t nao,
+                                   double sign, int beta0, double* __restrict__ K) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nao * nao) return;
+  const int64_t i = t / nao, j = t % nao;
+  const int64_t src = i >= j ? i * nao + j : j * nao + i;
+  double acc = 0.0;
+  for (int64_t s = 0; s < nsplit; ++s) acc += part[s * nao * nao + src];
+  K[t] = beta0 ? sign * acc : K[t] + sign * acc;
+}
+
 __global__ void scale_cols_kernel(const double* __restrict__ C, const double* __restrict__ w,
                                   int64_t nao, int64_t ncol, const int* __restrict__ sel,
                                   int64_t nsel, double* __restrict__ out) {
@@ -273,6 +359,36 @@ __global__ void symmetrize_kernel(double* __restrict__ K, int64_t n) {
   if (t >= n * n) return;
   const int64_t i = t / n, j = t % n;
   if (j < i) K[t] = K[j * n + i];
+}
+
+// K (+)= sign * X X^T (float64, full square) for X nao x kt row-major: lower
+// 64 x 64 tile pairs times k slices, enough blocks for several waves, then a
+// fixed-order sum of the slices (bit-reproducible).
+static void syrk_fp64(Plan& p, const double* X, int64_t kt, double sign, bool beta0, double* K,
+                      cudaStream_t s) {
+  const int64_t nao = p.nao;
+  const int64_t nt = (nao + kSyT - 1) / kSyT;
+  std::vector<int2> tl;
+  for (int64_t a = 0; a < nt; ++a)
+    for (int64_t b = 0; b <= a; ++b) tl.push_back(make_int2((int)a, (int)b));
+  int sm = 148;
+  cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, p.ctx->device);
+  const int64_t want = 4 * (int64_t)sm;
+  int64_t nsplit = std::max<int64_t>(1, (want + (int64_t)tl.size() - 1) / (int64_t)tl.size());
+  nsplit = std::min<int64_t>(nsplit, std::max<int64_t>(1, kt / 1024));
+  nsplit = std::min<int64_t>(nsplit, 65535);
+  const int64_t kslice = ((kt + nsplit - 1) / nsplit + kSyK - 1) / kSyK * kSyK;
+  nsplit = (kt + kslice - 1) / kslice;
+  p.ws_syrk_tiles.ensure(tl.size() * sizeof(int2));
+  DFJK_CUDA(cudaMemcpyAsync(p.ws_syrk_tiles.p, tl.data(), tl.size() * sizeof(int2),
+                            cudaMemcpyHostToDevice, s));
+  p.ws_syrk.ensure((size_t)nsplit * nao * nao * sizeof(double));
+  syrk_part_kernel<<<dim3((unsigned)tl.size(), (unsigned)nsplit), 256, 0, s>>>(
+      X, nao, kt, kslice, p.ws_syrk_tiles.as<int2>(), p.ws_syrk.as<double>());
+  DFJK_LAUNCHED();
+  syrk_reduce_kernel<<<(unsigned)((nao * nao + 255) / 256), 256, 0, s>>>(
+      p.ws_syrk.as<double>(), nsplit, nao, sign, beta0 ? 1 : 0, K);
+  DFJK_LAUNCHED();
 }
 
 // K (+)= sign * X X^T for the selected columns of C (scaled by sqrt|w|)
@@ -318,11 +434,7 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
     if (p.opts.precision == DFJK_MIXED) {
       ozaki_syrk(p, X.as<double>(), n * nsel, sign, beta0, K, s);   // full square, int8 tensor cores
     } else {
-      // X row-major (nao x n*nsel) == column-major (n*nsel x nao): K = op(A) op(A)^T, op = T
-      const double alpha = sign, beta = beta0 ? 0.0 : 1.0;
-      DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)nao,
-                              (int)(n * nsel), &alpha, X.as<double>(), (int)(n * nsel), &beta, K,
-                              (int)nao));
+      syrk_fp64(p, X.as<double>(), n * nsel, sign, beta0, K, s);
     }
     p.timer.mark(kPhKsyrk, s);
     beta0 = false;
