@@ -50,13 +50,16 @@ def df_k(int3c, vinv, Q):
     return np.einsum("mlP,PQ,nsQ,ls->mn", int3c, vinv, int3c, Q, optimize=True)
 
 
-def df_energy(int3c, vinv, P, hf_coeff):
-    """E_J + a_x E_K for the spin-stacked density P (nspin, nao, nao)."""
+def df_energy(int3c, vinv, P, hf_coeff, int3c_lr=None, vinv_lr=None, hf_coeff_lr=0.0):
+    """E_J + a_x E_K (+ a_lr E_K[erf(omega r)/r]) for the spin-stacked density P
+    (nspin, nao, nao): ``DFCoulomb.energy`` (terms.py:592-613)."""
     Ptot = P.sum(0)
     gamma = np.einsum("mnP,mn->P", int3c, Ptot)
     e = 0.5 * gamma @ (vinv @ gamma)
     if hf_coeff != 0.0:
         e = e + exchange_quadratic(lambda Q: df_k(int3c, vinv, Q), P, hf_coeff)
+    if hf_coeff_lr != 0.0:
+        e = e + exchange_quadratic(lambda Q: df_k(int3c_lr, vinv_lr, Q), P, hf_coeff_lr)
     return float(e)
 
 

@@ -112,12 +112,20 @@ def ec_table(lc, g, mt):
     return E
 
 
-def hermite_r(rho, pc, mt):
-    """(T, mt, mt, mt) R^0_{tuv} by the descending m-ladder."""
+def hermite_r(rho, pc, mt, omega=None):
+    """(T, mt, mt, mt) R^0_{tuv} by the descending m-ladder.
+
+    ``omega``: the long-range erf(omega r)/r operator, whose base values are
+    s^(m+1/2) F_m(s T) with s = omega^2 / (omega^2 + rho)
+    (``eri3c_bucketed.py:342-346``)."""
     T = rho.shape[0]
     targ = rho * np.einsum("ti,ti->t", pc, pc)
     m2r = -2.0 * rho
-    base = [m2r ** m * boys(m, targ) for m in range(mt)]
+    if omega is None:
+        base = [m2r ** m * boys(m, targ) for m in range(mt)]
+    else:
+        sat = omega * omega / (omega * omega + rho)
+        base = [m2r ** m * sat ** (m + 0.5) * boys(m, sat * targ) for m in range(mt)]
     R = np.zeros((T, mt, mt, mt))
     R[:, 0, 0, 0] = base[mt - 1]
     idx = np.arange(mt - 1, dtype=np.float64)
@@ -155,7 +163,7 @@ def _conv(Eab, Ec, mt):
 # 3-center (ab|c) for one class, cartesian, over a batch of triples
 # ---------------------------------------------------------------------------
 
-def _class_cart(la, lb, lc, anga, angb, angc, A, B, C, ea, eb, ec, ca, cb, cc):
+def _class_cart(la, lb, lc, anga, angb, angc, A, B, C, ea, eb, ec, ca, cb, cc, omega=None):
     """(T, nca, ncb, ncc) contracted cartesian integrals of one class."""
     mt = max(la + lb + lc + 1, 2)
     T = A.shape[0]
@@ -181,7 +189,7 @@ def _class_cart(la, lb, lc, anga, angb, angc, A, B, C, ea, eb, ec, ca, cb, cc):
                 gc = np.where(gc == 0.0, 1.0, gc)
                 rho = g * gc / (g + gc)
                 pref = K * TWO_PI_2_5 / (g * gc * np.sqrt(g + gc))
-                R = hermite_r(rho, P - C, mt)
+                R = hermite_r(rho, P - C, mt, omega)
                 Ec = ec_table(lc, gc, mt)
                 G = [_conv(Et[x], Ec, mt) for x in range(3)]
                 GX = G[0][:, ia[0][:, None, None], jb[0][None, :, None], kc[0][None, None, :], :]
@@ -234,19 +242,20 @@ def _gather(basis, sh, idx):
     return cen, ex, co, rows
 
 
-def eri3c(orb, aux, keep_pairs=None, chunk_elems=2_000_000):
-    """Dense (nao, nao, naux) spherical 3-center tensor (both bra triangles)."""
+def eri3c(orb, aux, keep_pairs=None, chunk_elems=2_000_000, omega=None):
+    """Dense (nao, nao, naux) spherical 3-center tensor (both bra triangles);
+    ``omega`` selects the erf(omega r)/r operator."""
     sb, sa = shells(orb), shells(aux)
     _, nao = sph_starts(sb, orb.cart2sph)
     _, naux = sph_starts(sa, aux.cart2sph)
     out = np.zeros((nao, nao, naux))
-    for ra, rb, rc, v in eri3c_blocks(orb, aux, keep_pairs, chunk_elems):
+    for ra, rb, rc, v in eri3c_blocks(orb, aux, keep_pairs, chunk_elems, omega):
         out[ra[:, :, None, None], rb[:, None, :, None], rc[:, None, None, :]] = v
         out[rb[:, None, :, None], ra[:, :, None, None], rc[:, None, None, :]] = v
     return out
 
 
-def eri3c_blocks(orb, aux, keep_pairs=None, chunk_elems=2_000_000):
+def eri3c_blocks(orb, aux, keep_pairs=None, chunk_elems=2_000_000, omega=None):
     """Yield (rows_a, rows_b, cols, values) per chunk of shell triples of one
     class: values[t] is the spherical (na, nb, nc) block of triple t, written at
     rows_a[t] x rows_b[t] x cols[t] of the dense tensor."""
@@ -269,7 +278,8 @@ def eri3c_blocks(orb, aux, keep_pairs=None, chunk_elems=2_000_000):
             A, ea, ca, _ = _gather(orb, sb, ia)
             B, eb, cb, _ = _gather(orb, sb, ib)
             C, ec, cc, _ = _gather(aux, sa, kc)
-            v = _class_cart(la, lb, lc, anga, angb, angc, A, B, C, ea, eb, ec, ca, cb, cc)
+            v = _class_cart(la, lb, lc, anga, angb, angc, A, B, C, ea, eb, ec, ca, cb, cc,
+                            omega)
             v = np.einsum("tabc,ap,bq,cr->tpqr", v, Ta, Tb, Tc)
             na, nb, nc = v.shape[1:]
             ra = sbs[ia][:, None] + np.arange(na)
@@ -282,8 +292,9 @@ def eri3c_blocks(orb, aux, keep_pairs=None, chunk_elems=2_000_000):
 # 2-center (P|Q)
 # ---------------------------------------------------------------------------
 
-def eri2c(aux):
-    """(naux, naux) spherical Coulomb metric (``eri3c_bucketed.py:697-779``)."""
+def eri2c(aux, omega=None):
+    """(naux, naux) spherical Coulomb metric (``eri3c_bucketed.py:697-779``);
+    ``omega`` selects the erf(omega r)/r operator."""
     sa = shells(aux)
     ang = np.asarray(aux.angular)
     ncart = ang.shape[0]
@@ -314,7 +325,7 @@ def eri2c(aux):
                     pref = TWO_PI_2_5 / (al * be * np.sqrt(al + be))
                     Ea = ec_table(la, al, mt)
                     Eb = ec_table(lb, be, mt) * sign
-                    R = hermite_r(rho, A - B, mt)
+                    R = hermite_r(rho, A - B, mt, omega)
                     G = np.zeros((T, la + 1, lb + 1, mt))
                     for t in range(mt):
                         for tau in range(mt - t):

@@ -21,7 +21,8 @@ is computed by the reference's unmodified functions:
 
 J is the analytic P-gradient of the RI-J energy, ``J = int3c . (V+ gamma)``,
 formed here from the reference's ``int3c`` and ``V+``; K is the reference's
-``df_k_matrix``. Outputs: ``boys_ref.npz``, ``water_ref.npz``, ``ch2_ref.npz``.
+``df_k_matrix``. Outputs: ``boys_ref.npz``, ``water_ref.npz``, ``water_rsh_ref.npz``
+(the range-separated erf(omega r)/r form), ``ch2_ref.npz``.
 The fixtures are read by the tests only; nothing at run time needs the
 reference.
 """
@@ -196,6 +197,40 @@ def make_system(R, name, sym, xyz, nocc, out, seed, sample=None, screen=None):
           f"E={e_total:.12f}", flush=True)
 
 
+def make_rsh(R, out, omega=0.3, hf=0.2, hf_lr=0.8, seed=0, nocc=5):
+    """Range-separated form of the water monomer: the erf(omega r)/r 3-center
+    tensor and metric (``eri3c_matrix_bucketed(..., omega=)``,
+    ``eri2c_matrix_bucketed(..., omega=)``), their pseudo-inverse, the
+    long-range K and the DFCoulomb energy with both exchange terms."""
+    t0 = time.time()
+    sym, xyz = systems.water_monomer()
+    orb = R.loader.build_basis_data(sym, xyz, "even-tempered-orbital", spherical=True)
+    aux = R.loader.build_basis_data(sym, xyz, "even-tempered-aux", spherical=True)
+    plan = R.eb.plan_eri3c(orb, aux)
+    int3c = np.asarray(R.eb.eri3c_matrix_bucketed(orb, aux, plan=plan))
+    int3c_lr = np.asarray(R.eb.eri3c_matrix_bucketed(orb, aux, omega=omega, plan=plan))
+    int2c = np.asarray(R.eb.eri2c_matrix_bucketed(aux))
+    int2c_lr = np.asarray(R.eb.eri2c_matrix_bucketed(aux, omega=omega))
+    vinv = np.asarray(R.terms._metric_pinv(int2c))
+    vinv_lr = np.asarray(R.terms._metric_pinv(int2c_lr))
+    nao = int3c.shape[0]
+    rng = np.random.default_rng(seed)
+    C, _ = np.linalg.qr(rng.standard_normal((nao, nocc)))
+    D = C @ C.T
+    P = 2.0 * D
+    dfc = R.terms.DFCoulomb(int3c=int3c, int2c_inv=vinv, hf_coeff=hf, int3c_lr=int3c_lr,
+                            int2c_inv_lr=vinv_lr, hf_coeff_lr=hf_lr)
+    e_total = float(dfc.energy(P[None], None, (nocc,)))
+    K_lr = np.asarray(R.hybrid.df_k_matrix(D, int3c_lr, vinv_lr))
+    w = np.linalg.eigvalsh(int2c_lr)
+    pa, pb = np.tril_indices(nao)
+    np.savez(out, omega=omega, hf_coeff=hf, hf_coeff_lr=hf_lr, C=C, e_total=e_total,
+             int3c_lr_tril=int3c_lr[pa, pb, :], int2c_lr=int2c_lr, vinv_lr=vinv_lr,
+             K_lr=K_lr, metric_w_lr=w, n_kept_lr=int(np.sum(w > 1e-7 * w[-1])))
+    print(f"water_rsh: omega={omega} E={e_total:.12f} kept={int(np.sum(w > 1e-7 * w[-1]))} "
+          f"{time.time() - t0:.1f}s", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -208,6 +243,8 @@ def main():
         sym, xyz = systems.water_monomer()
         make_system(R, "water", sym, xyz, 5, os.path.join(HERE, "water_ref.npz"), seed=0,
                     screen=1e-3)
+    if a.only in (None, "water_rsh"):
+        make_rsh(R, os.path.join(HERE, "water_rsh_ref.npz"))
     if a.only in (None, "ch2"):
         ang = systems.ANGSTROM_TO_BOHR
         s = 1.09 / np.sqrt(3.0)
