@@ -26,7 +26,7 @@ EXPORTS = (
     "dfjk_plan_create", "dfjk_plan_destroy", "dfjk_plan_get_info", "dfjk_build", "dfjk_jk",
     "dfjk_jk_host", "dfjk_energy", "dfjk_eri3c_dense", "dfjk_eri2c_dense", "dfjk_metric_pinv",
     "dfjk_kept_pairs", "dfjk_boys", "dfjk_phase_times", "dfjk_kernel_launches",
-    "dfjk_j_noalloc", "dfjk_trim",
+    "dfjk_j_noalloc", "dfjk_trim", "dfjk_plan_long_range", "dfjk_energy_rsh",
 )
 PHASES = ("metric", "pairs", "eri3c", "bgemm", "j", "khalf", "ksyrk", "kplanes")
 
@@ -52,7 +52,7 @@ class Basis(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("screen", c_double), ("metric_cutoff", c_double), ("precision", c_int32),
-                ("reserved", c_int32), ("chunk_bytes", c_int64)]
+                ("reserved", c_int32), ("chunk_bytes", c_int64), ("omega", c_double)]
 
 
 class PlanInfo(ctypes.Structure):
@@ -99,6 +99,8 @@ def load(path: str | None = None):
         "dfjk_kernel_launches": (c_int64, []),
         "dfjk_j_noalloc": (c_int, [V, V, V, c_int64, V, V]),
         "dfjk_trim": (c_int, [V]),
+        "dfjk_plan_long_range": (c_int, [V, P(c_void_p)]),
+        "dfjk_energy_rsh": (c_int, [V, V, c_int32, c_double, c_double, P(c_double), V, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -108,7 +108,7 @@ class Plan:
 
     def __init__(self, orb: BasisData, aux: BasisData, *, screen: float | None = None,
                  precision: str = "fp64", metric_cutoff: float = 1e-7, chunk_bytes: int = 0,
-                 device: int = 0, ctx: Context | None = None):
+                 omega: float = 0.0, device: int = 0, ctx: Context | None = None):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         self.ctx = ctx or Context.get(device)
@@ -123,6 +123,9 @@ class Plan:
         opts.metric_cutoff = float(metric_cutoff)
         opts.precision = PRECISIONS[precision]
         opts.chunk_bytes = int(chunk_bytes)
+        opts.omega = float(omega)
+        self.omega = float(omega)
+        self._parent = None
         self.h = ctypes.c_void_p()
         check(self.lib.dfjk_plan_create(self.ctx.h, byref(ob), byref(ab), byref(opts),
                                         byref(self.h)), self.ctx.h)
@@ -130,9 +133,24 @@ class Plan:
 
     # -- lifecycle -------------------------------------------------------
     def close(self):
+        if getattr(self, "_parent", None) is not None:   # owned by the parent plan
+            self.h = ctypes.c_void_p()
+            return
         if getattr(self, "h", None) and self.h.value:
             self.lib.dfjk_plan_destroy(self.h)
             self.h = ctypes.c_void_p()
+
+    @property
+    def long_range(self) -> "Plan":
+        """The erf(omega r)/r plan of a plan made with omega > 0 (built by this
+        plan's ``build``): its ``jk`` gives K_lr, its diagnostics the
+        attenuated tensors. Valid while this plan lives."""
+        h = ctypes.c_void_p()
+        check(self.lib.dfjk_plan_long_range(self.h, byref(h)), self.ctx.h)
+        lr = Plan.__new__(Plan)
+        lr.ctx, lr.lib, lr.torch, lr.dev = self.ctx, self.lib, self.torch, self.dev
+        lr.precision, lr.omega, lr._parent, lr.h = self.precision, self.omega, self, h
+        return lr
 
     def __del__(self):  # pragma: no cover - best effort
         try:
@@ -199,8 +217,10 @@ class Plan:
                                     _stream_ptr(self.torch, stream)), self.ctx.h)
         return J, K
 
-    def energy(self, P, hf_coeff: float, *, want_grad: bool = True, stream=None):
-        """(E, dE/dP) of DFCoulomb.energy for the spin-stacked density P."""
+    def energy(self, P, hf_coeff: float, *, hf_coeff_lr: float = 0.0, want_grad: bool = True,
+               stream=None):
+        """(E, dE/dP) of DFCoulomb.energy for the spin-stacked density P;
+        ``hf_coeff_lr`` adds the long-range exchange (plans made with omega)."""
         t = self.torch
         P = self._dev(P)
         if P.ndim == 2:
@@ -208,9 +228,10 @@ class Plan:
         nspin = P.shape[0]
         F = t.empty_like(P) if want_grad else None
         e = ctypes.c_double()
-        check(self.lib.dfjk_energy(self.h, P.data_ptr(), nspin, float(hf_coeff), byref(e),
-                                   None if F is None else F.data_ptr(),
-                                   _stream_ptr(t, stream)), self.ctx.h)
+        check(self.lib.dfjk_energy_rsh(self.h, P.data_ptr(), nspin, float(hf_coeff),
+                                       float(hf_coeff_lr), byref(e),
+                                       None if F is None else F.data_ptr(),
+                                       _stream_ptr(t, stream)), self.ctx.h)
         return e.value, F
 
     # -- parity entry points --------------------------------------------
@@ -290,34 +311,42 @@ class B200DFCoulomb(CoulombTerm):
     Same energy as ``DFCoulomb.energy`` (``terms.py:592-613``):
     ``E = 1/2 gamma^T V+ gamma - 1/4 a_x Tr(P K(P))`` for one channel,
     ``- 1/2 a_x sum_s Tr(P_s K(P_s))`` for two; ``fock`` adds its P-gradient.
+    Range-separated hybrids (``hf_coeff_lr`` with ``omega``) add the same
+    exchange quadratic of the erf(omega r)/r fit (``terms.py:604-612``).
     """
 
     def __init__(self, basis: BasisData, aux_basis: BasisData, hf_coeff: float, *,
-                 screen: float | None = None, precision: str = "fp64", device: int = 0):
+                 hf_coeff_lr: float = 0.0, omega: float = 0.0, screen: float | None = None,
+                 precision: str = "fp64", device: int = 0):
+        if hf_coeff_lr != 0.0 and omega <= 0.0:
+            raise ValueError("hf_coeff_lr needs omega > 0 (terms.py:953-978)")
         self.hf_coeff = float(hf_coeff)
-        self.plan = Plan(basis, aux_basis, screen=screen, precision=precision, device=device)
+        self.hf_coeff_lr = float(hf_coeff_lr)
+        self.plan = Plan(basis, aux_basis, screen=screen, precision=precision,
+                         omega=omega if hf_coeff_lr != 0.0 else 0.0, device=device)
         self.plan.build()
 
     def energy(self, P, S=None, nocc=None) -> float:
-        e, _ = self.plan.energy(P, self.hf_coeff, want_grad=False)
+        e, _ = self.plan.energy(P, self.hf_coeff, hf_coeff_lr=self.hf_coeff_lr, want_grad=False)
         return e
 
     def fock(self, P, S=None, nocc=None):
         """(E, dE/dP) with dE/dP on the device, shaped like P."""
-        return self.plan.energy(P, self.hf_coeff, want_grad=True)
+        return self.plan.energy(P, self.hf_coeff, hf_coeff_lr=self.hf_coeff_lr, want_grad=True)
 
     def jk(self, C, w=None):
         return self.plan.jk(C, w)
 
 
-def make_coulomb(spec: DFSpec, basis: BasisData, hf_coeff: float, *, device: int = 0):
+def make_coulomb(spec: DFSpec, basis: BasisData, hf_coeff: float, *, hf_coeff_lr: float = 0.0,
+                 omega: float = 0.0, device: int = 0):
     """``_make_coulomb`` (``terms.py:951-988``) for a resolved b200 spec."""
     if not isinstance(spec, DFSpec):
         raise TypeError("make_coulomb expects a DFSpec from dftax_b200.df()")
     if not isinstance(spec.auxbasis, BasisData):
         raise TypeError("spec.auxbasis must be a built BasisData")
-    return B200DFCoulomb(basis, spec.auxbasis, hf_coeff, screen=spec.screen,
-                         precision=spec.precision, device=device)
+    return B200DFCoulomb(basis, spec.auxbasis, hf_coeff, hf_coeff_lr=hf_coeff_lr, omega=omega,
+                         screen=spec.screen, precision=spec.precision, device=device)
 
 
 __all__ = ["Context", "Plan", "DFSpec", "df", "CoulombTerm", "B200DFCoulomb", "make_coulomb"]

@@ -794,7 +794,8 @@ void metric_pinv(Plan& p, double* out, cudaStream_t s) {
   DFJK_CUDA(cudaStreamSynchronize(s));
 }
 
-double energy(Plan& p, const double* P, int nspin, double hf, double* F, cudaStream_t s);
+double energy(Plan& p, const double* P, int nspin, double hf, double hf_lr, double* F,
+              cudaStream_t s);
 
 }  // namespace dfjk
 
@@ -890,7 +891,20 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
       fail(DFJK_ERR_INVALID, "invalid options");
     if (pl->p.opts.precision != DFJK_FP64 && pl->p.opts.precision != DFJK_MIXED)
       fail(DFJK_ERR_INVALID, "unknown precision %d", pl->p.opts.precision);
+    if (!(pl->p.opts.omega >= 0.0) || !std::isfinite(pl->p.opts.omega))
+      fail(DFJK_ERR_INVALID, "omega must be finite and >= 0");
     make_plan(pl->p, orb, aux);
+    if (pl->p.opts.omega > 0.0) {
+      // the long-range operator over the same bases; its Schwarz screen is the
+      // same full-range one, so it keeps the same shell pairs
+      dfjk_plan* lr = new dfjk_plan;
+      pl->p.lr = lr;
+      lr->p.ctx = &h->c;
+      lr->p.opts = pl->p.opts;
+      lr->p.atten = pl->p.opts.omega;
+      lr->p.owned_by_parent = true;
+      make_plan(lr->p, orb, aux);
+    }
     // the int8 products are exact for dot products of at most kOzMaxK terms
     if (pl->p.opts.precision == DFJK_MIXED &&
         (pl->p.naux > kOzMaxK || pl->p.nao > kOzMaxK))
@@ -898,6 +912,7 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
            (long long)kOzMaxK, pl->p.nao, pl->p.naux);
   });
   if (r != DFJK_OK) {
+    delete pl->p.lr;
     delete pl;
     return r;
   }
@@ -907,10 +922,12 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
 
 dfjk_status dfjk_plan_destroy(dfjk_plan* pl) {
   if (!pl) return DFJK_OK;
+  if (pl->p.owned_by_parent) return DFJK_ERR_INVALID;   // freed with its parent
   const int dev = pl->p.ctx->device;
   cudaSetDevice(dev);
   // work queued on the plan's buffers ends here; they go back to the cache idle
   cudaDeviceSynchronize();
+  delete pl->p.lr;
   delete pl;
   dfjk::device_synchronized(dev);
   return DFJK_OK;
@@ -947,7 +964,14 @@ dfjk_status dfjk_build(dfjk_plan* pl, void* stream) {
   return guard(pl->p.ctx, [&] {
     DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
     build(pl->p, st(stream));
+    if (pl->p.lr) build(pl->p.lr->p, st(stream));
   });
+}
+
+dfjk_status dfjk_plan_long_range(const dfjk_plan* pl, dfjk_plan** lr) {
+  if (!pl || !lr) return DFJK_ERR_INVALID;
+  *lr = pl->p.lr;
+  return pl->p.lr ? DFJK_OK : DFJK_ERR_STATE;
 }
 
 dfjk_status dfjk_jk(dfjk_plan* pl, const double* C, const double* w, int64_t ncol, double* J,
@@ -990,13 +1014,23 @@ dfjk_status dfjk_jk_host(dfjk_plan* pl, const double* C, const double* w, int64_
 
 dfjk_status dfjk_energy(dfjk_plan* pl, const double* P, int32_t nspin, double hf_coeff, double* e,
                         double* F, void* stream) {
+  return dfjk_energy_rsh(pl, P, nspin, hf_coeff, 0.0, e, F, stream);
+}
+
+dfjk_status dfjk_energy_rsh(dfjk_plan* pl, const double* P, int32_t nspin, double hf_coeff,
+                            double hf_coeff_lr, double* e, double* F, void* stream) {
   if (!pl) return DFJK_ERR_INVALID;
   return guard(pl->p.ctx, [&] {
     if (!pl->p.built) fail(DFJK_ERR_STATE, "dfjk_energy before dfjk_build");
     if (!P || !e || (nspin != 1 && nspin != 2)) fail(DFJK_ERR_INVALID, "bad energy arguments");
-    if (!std::isfinite(hf_coeff)) fail(DFJK_ERR_INVALID, "non-finite hf_coeff");
+    if (!std::isfinite(hf_coeff) || !std::isfinite(hf_coeff_lr))
+      fail(DFJK_ERR_INVALID, "non-finite exchange coefficient");
+    if (hf_coeff_lr != 0.0 && !pl->p.lr)
+      fail(DFJK_ERR_STATE, "hf_coeff_lr needs a plan made with omega > 0");
+    if (hf_coeff_lr != 0.0 && !pl->p.lr->p.built)
+      fail(DFJK_ERR_STATE, "the long-range plan is not built");
     DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
-    *e = energy(pl->p, P, nspin, hf_coeff, F, st(stream));
+    *e = energy(pl->p, P, nspin, hf_coeff, hf_coeff_lr, F, st(stream));
   });
 }
 

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
     const double rho = g * gc / (g + gc);
     const double X = P0 - C0, Y = P1 - C1, Z = P2 - C2;
     double F[M + 1];
-    boys_eval<M>(rho * (X * X + Y * Y + Z * Z), a.boys, a.boys_asym, F);
+    boys_operator<M>(rho * (X * X + Y * Y + Z * Z), rho, a.omega, a.boys, a.boys_asym, F);
     double R[NR];
     hermite_r<M>(rho, X, Y, Z, F, R);
     double hob = 1.0;
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
       const double rho = g * gc / (g + gc);
       const double X = P0 - C0, Y = P1 - C1, Z = P2 - C2;
       double F[M + 1];
-      boys_eval<M>(rho * (X * X + Y * Y + Z * Z), a.boys, a.boys_asym, F);
+      boys_operator<M>(rho * (X * X + Y * Y + Z * Z), rho, a.omega, a.boys, a.boys_asym, F);
       double R[NR];
       hermite_r<M>(rho, X, Y, Z, F, R);
       double hob = 1.0;

@@ -170,6 +170,13 @@ struct ClassRange {   // a contiguous run of shell pairs of one (l1, l2) class
 struct Plan {
   Context* ctx = nullptr;
   dfjk_options opts{};
+  // operator of this plan's integrals: 0 = Coulomb, > 0 = erf(atten r)/r
+  double atten = 0.0;
+  // range-separated plans (opts.omega > 0) own a second plan for the
+  // long-range operator over the same bases and shell pairs; it is built with
+  // this one and freed with it
+  dfjk_plan* lr = nullptr;
+  bool owned_by_parent = false;
   Shells orb, aux;
   Blocks c2s_orb, c2s_aux;
   int nao = 0, naux = 0;

@@ -531,7 +531,9 @@ static double dot(const double* a, const double* b, int64_t n, cudaStream_t s) {
 
 // K of a symmetric density Q (device, nao x nao): Q = V diag(l) V^T on the
 // device, K(Q) = sum_k l_k K(v_k v_k^T) over |l_k| > 1e-14 max|l|.
-static void k_of_density(Plan& p, const double* Q, double* K, cudaStream_t s) {
+// Eigen-factor of a symmetric Q (nao x nao): Ct row-major with Q = Ct diag(dw) Ct^T,
+// eigenvalues below 1e-14 of the largest set to zero, so K(Q) = k_compute(Ct, dw).
+static void density_factor(Plan& p, const double* Q, DevBuf& Ct, DevBuf& dw, cudaStream_t s) {
   Context& c = *p.ctx;
   const int64_t n = p.nao;
   DevBuf V, wv, work, info;
@@ -558,7 +560,6 @@ static void k_of_density(Plan& p, const double* Q, double* K, cudaStream_t s) {
   for (double v : hw) big = std::max(big, std::fabs(v));
   // eigenvectors are the columns of the column-major V, i.e. rows of the
   // row-major view: C[m][k] = V[k*n + m]; transpose into a row-major C
-  DevBuf Ct;
   Ct.alloc((size_t)n * n * sizeof(double));
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
   const double one = 1.0, zero = 0.0;
@@ -567,12 +568,13 @@ static void k_of_density(Plan& p, const double* Q, double* K, cudaStream_t s) {
   std::vector<double> wsel(n, 0.0);
   for (int64_t k = 0; k < n; ++k)
     if (std::fabs(hw[k]) > 1e-14 * big) wsel[k] = hw[k];
-  DevBuf dw;
   upload(dw, wsel);
-  k_compute(p, Ct.as<double>(), dw.as<double>(), n, K, s);
 }
 
-double energy(Plan& p, const double* P, int nspin, double hf, double* F, cudaStream_t s) {
+// hf_lr: the long-range exchange of range-separated hybrids through the plan's
+// long-range fit (terms.py:604-612)
+double energy(Plan& p, const double* P, int nspin, double hf, double hf_lr, double* F,
+              cudaStream_t s) {
   const int64_t n = p.nao, nn = n * n;
   DevBuf Ptot, dvec, gamma, J;
   const double* Pt = P;
@@ -599,19 +601,26 @@ double energy(Plan& p, const double* P, int nspin, double hf, double* F, cudaStr
     for (int sp = 0; sp < nspin; ++sp)
       DFJK_CUDA(cudaMemcpyAsync(F + sp * nn, J.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
   }
-  if (hf != 0.0) {
-    DevBuf K;
+  if (hf != 0.0 || hf_lr != 0.0) {
+    DevBuf K, Ct, dw;
     K.alloc(nn * sizeof(double));
     for (int sp = 0; sp < nspin; ++sp) {
       const double* Ps = P + sp * nn;
-      k_of_density(p, Ps, K.as<double>(), s);
-      const double tr = dot(Ps, K.as<double>(), nn, s);
-      // exchange quadratic (terms.py:500-509)
-      e += (nspin == 1 ? -0.25 : -0.5) * hf * tr;
-      if (F) {
-        const double a = (nspin == 1 ? -0.5 : -1.0) * hf;
-        axpy_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(K.as<double>(), a, nn, F + sp * nn);
-        DFJK_LAUNCHED();
+      density_factor(p, Ps, Ct, dw, s);
+      const struct { Plan* plan; double coeff; } terms[2] = {{&p, hf},
+                                                             {p.lr ? &p.lr->p : nullptr, hf_lr}};
+      for (const auto& t : terms) {
+        if (t.coeff == 0.0) continue;
+        k_compute(*t.plan, Ct.as<double>(), dw.as<double>(), n, K.as<double>(), s);
+        const double tr = dot(Ps, K.as<double>(), nn, s);
+        // exchange quadratic (terms.py:500-509)
+        e += (nspin == 1 ? -0.25 : -0.5) * t.coeff * tr;
+        if (F) {
+          const double a = (nspin == 1 ? -0.5 : -1.0) * t.coeff;
+          axpy_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(K.as<double>(), a, nn,
+                                                                    F + sp * nn);
+          DFJK_LAUNCHED();
+        }
       }
     }
   }

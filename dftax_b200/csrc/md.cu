@@ -191,6 +191,7 @@ struct Eri2cArgs {
   int colP, colQ;                       // first columns of the groups
   int64_t ld;
   double* out;
+  double omega;                         // > 0: erf(omega r)/r operator
 };
 
 template <int LP, int LQ>
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(128) eri2c_kernel(Eri2cArgs a) {
       const double be = a.aux.pexp[a.aux.prim0[sq] + j], cb = a.aux.pcoef[a.aux.prim0[sq] + j];
       const double rho = al * be / (al + be);
       double F[M + 1];
-      boys_eval<M>(rho * (X * X + Y * Y + Z * Z), a.boys, a.boys_asym, F);
+      boys_operator<M>(rho * (X * X + Y * Y + Z * Z), rho, a.omega, a.boys, a.boys_asym, F);
       double R[NR];
       hermite_r<M>(rho, X, Y, Z, F, R);
       double hob = kTwoPi25 * ca * cb / (al * be * sqrt(al + be));
@@ -434,6 +435,7 @@ void launch_eri3c_rows(Plan& p, int64_t pair_begin, int64_t pair_end, int64_t ro
       a.ld = ld;
       a.out = out;
       a.out_f32 = f32 ? 1 : 0;
+      a.omega = p.atten;
       const int ychunks = (a.aux_count + 127) / 128;
       for (int64_t q = b; q < e; q += (int64_t)1 << 30) {
         const int64_t n = (e - q) < ((int64_t)1 << 30) ? (e - q) : ((int64_t)1 << 30);
@@ -464,6 +466,7 @@ void launch_eri2c(Plan& p, double* out, int64_t ld, cudaStream_t s) {
       a.offP = p.c2s_aux.off[lp];
       a.offQ = p.c2s_aux.off[lq];
       a.boys = c.boys.as<double>();
+      a.omega = p.atten;
       a.boys_asym = c.boys_asym.as<double>();
       a.beginP = p.aux_lbegin[lp];
       a.countP = p.aux_lcount[lp];

@@ -62,6 +62,28 @@ __device__ __forceinline__ void boys_eval(double t, const double* __restrict__ t
   }
 }
 
+// Boys values of the Hermite base for the Coulomb operator (omega == 0) or
+// the long-range erf(omega r)/r operator (omega > 0): with
+// s = omega^2 / (omega^2 + rho), F_m(t) becomes s^(m+1/2) F_m(s t)
+// (dftax/integrals/eri3c_bucketed.py:342-346).
+template <int M>
+__device__ __forceinline__ void boys_operator(double t, double rho, double omega,
+                                              const double* __restrict__ tbl,
+                                              const double* __restrict__ asym, double (&F)[M + 1]) {
+  if (omega > 0.0) {
+    const double s = omega * omega / (omega * omega + rho);
+    boys_eval<M>(s * t, tbl, asym, F);
+    double f = sqrt(s);
+#pragma unroll
+    for (int n = 0; n <= M; ++n) {
+      F[n] *= f;
+      f *= s;
+    }
+  } else {
+    boys_eval<M>(t, tbl, asym, F);
+  }
+}
+
 // Hermite R^0_{tuv}, t+u+v <= M, packed by hidx, in place over the levels
 // m = M..0 from R^m_000 = (-2 rho)^m F_m. At level m the entries of total
 // order k are updated in descending k, so the orders k-1 and k-2 they read
@@ -165,6 +187,7 @@ struct Eri3cArgs {
   int64_t ld;
   void* out;
   int out_f32;               // 1: float output, 0: double
+  double omega;              // > 0: erf(omega r)/r operator
 };
 
 

@@ -66,6 +66,8 @@ typedef struct {
   int32_t precision;    /* DFJK_FP64 or DFJK_MIXED                               */
   int32_t reserved;
   int64_t chunk_bytes;  /* staging budget for raw 3-center rows (0 = default)   */
+  double omega;         /* > 0: also build the long-range erf(omega r)/r fit for
+                           range-separated exchange (energy.py:419-433); 0: off */
 } dfjk_options;
 
 typedef struct {
@@ -80,7 +82,7 @@ typedef struct {
   int32_t precision;
 } dfjk_plan_info;
 
-/* Fill opts with dftax's defaults: screen off, cutoff 1e-7, FP64. */
+/* Fill opts with dftax's defaults: screen off, cutoff 1e-7, FP64, omega 0. */
 void dfjk_default_options(dfjk_options* opts);
 
 /* Context: device, library handles and the Boys table (dftax/energy/boys.py:81-123). */
@@ -123,6 +125,14 @@ dfjk_status dfjk_jk(dfjk_plan* plan, const double* C, const double* w, int64_t n
 dfjk_status dfjk_jk_host(dfjk_plan* plan, const double* C, const double* w, int64_t ncol,
                          double* J, double* K, void* stream);
 
+/* The long-range plan of a plan made with omega > 0: the erf(omega r)/r
+ * 3-center tensor and metric (eri3c_bucketed.py:746-854 with omega), its own
+ * pseudo-inverse and factor, B_lr (int3c_lr / int2c_inv_lr of energy.py:419-433).
+ * Owned by the parent (built by the parent's dfjk_build, freed with it;
+ * dfjk_plan_destroy refuses it). dfjk_jk on it gives K_lr (and the long-range
+ * J); the diagnostics give the attenuated tensors. DFJK_ERR_STATE without omega. */
+dfjk_status dfjk_plan_long_range(const dfjk_plan* plan, dfjk_plan** lr);
+
 /* DFCoulomb.energy (terms.py:592-613) and its P-gradient for the spin-stacked
  * density P [nspin][nao][nao] (device): energy -> *e (host scalar) and, when
  * F != NULL, dE/dP -> F [nspin][nao][nao] (device): J - a_x/2 K for nspin 1,
@@ -130,6 +140,13 @@ dfjk_status dfjk_jk_host(dfjk_plan* plan, const double* C, const double* w, int6
  * exactly (it is diagonalized on the device). Host-synchronizing. */
 dfjk_status dfjk_energy(dfjk_plan* plan, const double* P, int32_t nspin, double hf_coeff,
                         double* e, double* F, void* stream);
+
+/* The same with the long-range exchange term of range-separated hybrids
+ * (terms.py:604-612): E += exchange quadratic of K_lr with hf_coeff_lr, and
+ * dE/dP gains -hf_coeff_lr/2 K_lr (nspin 1) or -hf_coeff_lr K_lr,sigma
+ * (nspin 2). hf_coeff_lr != 0 needs a plan made with omega > 0. */
+dfjk_status dfjk_energy_rsh(dfjk_plan* plan, const double* P, int32_t nspin, double hf_coeff,
+                            double hf_coeff_lr, double* e, double* F, void* stream);
 
 /* J of D = C diag(w) C^T, as dfjk_jk computes it, without allocating any
  * device memory: for callers that must not call cudaMalloc while they run
