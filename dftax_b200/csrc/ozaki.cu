@@ -408,8 +408,15 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
   a.ld_out = n * nsel;
   a.batch_stride_out = nsel;
   a.err = p.ws_oz_err.as<int>();
-  for (int64_t z0 = 0; z0 < n; z0 += 65535) {
-    const int64_t nz = std::min<int64_t>(65535, n - z0);
+  // several fitted directions per CTA (one TMEM allocation and one copy ring
+  // for all of them) while the grid still fills the device four times over
+  int sm = 148;
+  cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, p.ctx->device);
+  const int64_t tiles = ((nsel + sh.bn - 1) / sh.bn) * ((nao + 127) / 128);
+  a.zper = (int)std::max<int64_t>(1, std::min<int64_t>(16, tiles * n / (4 * (int64_t)sm)));
+  const int64_t zstep = (int64_t)65535 * a.zper;
+  for (int64_t z0 = 0; z0 < n; z0 += zstep) {
+    const int64_t nz = std::min<int64_t>(zstep, n - z0);
     a.plane0 = (int)(x0 + z0);
     a.out = X + z0 * nsel;
     ozaki_launch(kOzHalf, maps, a, (int)nz, s);

@@ -40,6 +40,8 @@ struct OzakiArgs {
   double* out;             // out[z * batch_stride + row * ld + col]
   int64_t ld_out, batch_stride_out;
   int* err;                // set non-zero when a bounded wait gives up
+  int zper;                // batches per CTA (one TMEM allocation, one ring); 0 or 1: one
+  int zcount;              // batches of the launch (set by ozaki_launch)
 };
 
 // 3-D int8 tensor map over [d2][d1][d0] (d0 contiguous; strides in bytes),
@@ -47,7 +49,7 @@ struct OzakiArgs {
 void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
                int64_t stride1, int64_t stride2, int box_k, int box1);
 
-// grid (ceil(N/bn), ceil(M/128), grid_z)
+// grid (ceil(N/bn), ceil(M/128), ceil(nbatch / a.zper)): nbatch batches (grid_z)
 void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, int grid_z,
                   cudaStream_t s);
 

@@ -136,7 +136,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v) {
 }
 
 template <int ND, int BK, int BN, int ST>
-__global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ OzakiMaps maps,
+__global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ OzakiMaps maps,
                                                         OzakiArgs a) {
   constexpr uint32_t A_TILE = kBM * BK;
   constexpr uint32_t B_TILE = BN * BK;
@@ -152,19 +152,27 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + ST * STAGE);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * ST + 1);
+  // barriers: full[ST], empty[ST], done (accumulators of a batch final),
+  // drained (the epilogue warps have read them)
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * STAGE);
+  uint64_t* empty = full + ST;
+  uint64_t* done = empty + ST;
+  uint64_t* drained = done + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * kBM, z = blockIdx.z;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * kBM;
   const int nk = a.ktiles;
-  const int bz = a.b_batched ? a.plane0 + z : 0;   // B plane (and exponent set) of this CTA
+  const int zper = a.zper > 0 ? a.zper : 1;
+  const int z0 = blockIdx.z * zper;
+  const int nz = (a.zcount - z0) < zper ? (a.zcount - z0) : zper;   // batches of this CTA
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) {
-      mbar_init(smem_u32(&bars[s]), 1);
-      mbar_init(smem_u32(&bars[ST + s]), 1);
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
     }
-    mbar_init(smem_u32(&bars[2 * ST]), 1);
+    mbar_init(smem_u32(done), 1);
+    mbar_init(smem_u32(drained), 4);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -181,96 +189,112 @@ __global__ void __launch_bounds__(128, 1) ozaki_gemm_i8(const __grid_constant__ 
   const uint32_t tmem = *tmem_slot;
 
   if (threadIdx.x == 0 && nk > 0) {
+    // producer: the k tiles of every batch of this CTA through one ring
     int issued = 0;
     bool ok = true;
-    for (int i = 0; i < nk && ok; ++i) {
-      const int s = i % ST;
-      if (i >= ST) ok = mbar_wait(smem_u32(&bars[ST + s]), ((i / ST) - 1) & 1, a.err, 1);
-      if (!ok) break;
-      const uint32_t full = smem_u32(&bars[s]);
-      mbar_expect_tx(full, STAGE);
-      uint8_t* st = smem + s * STAGE;
+    for (int zi = 0; zi < nz && ok; ++zi) {
+      const int z = z0 + zi;
+      const int bz = a.b_batched ? a.plane0 + z : 0;
+      for (int i = 0; i < nk; ++i, ++issued) {
+        const int s = issued % ST;
+        if (issued >= ST) ok = mbar_wait(smem_u32(&empty[s]), ((issued / ST) - 1) & 1, a.err, 1);
+        if (!ok) break;
+        const uint32_t fb = smem_u32(&full[s]);
+        mbar_expect_tx(fb, STAGE);
+        uint8_t* st = smem + s * STAGE;
 #pragma unroll
-      for (int d = 0; d < ND; ++d) {
-        tma_load_3d(smem_u32(st + d * A_TILE), &maps.a[d], full, i * BK, m0, a.plane0 + z);
-        tma_load_3d(smem_u32(st + ND * A_TILE + d * B_TILE), &maps.b[d], full, i * BK, n0, bz);
+        for (int d = 0; d < ND; ++d) {
+          tma_load_3d(smem_u32(st + d * A_TILE), &maps.a[d], fb, i * BK, m0, a.plane0 + z);
+          tma_load_3d(smem_u32(st + ND * A_TILE + d * B_TILE), &maps.b[d], fb, i * BK, n0, bz);
+        }
       }
-      ++issued;
     }
     if (!ok) {
-      for (int i = issued - ST > 0 ? issued - ST : 0; i < issued; ++i) {
+      for (int q = issued - ST > 0 ? issued - ST : 0; q < issued; ++q) {
         const uint64_t t0 = now_ns();
-        while (!mbar_try(smem_u32(&bars[i % ST]), (i / ST) & 1) && now_ns() - t0 < kWaitNs)
+        while (!mbar_try(smem_u32(&full[q % ST]), (q / ST) & 1) && now_ns() - t0 < kWaitNs)
           __nanosleep(64);
       }
     }
   } else if (threadIdx.x == 32 && nk > 0) {
+    // MMA issuer: one accumulator set per batch, reused once the epilogue drained it
     bool ok = true;
-    for (int i = 0; i < nk; ++i) {
-      const int s = i % ST;
-      ok = mbar_wait(smem_u32(&bars[s]), (i / ST) & 1, a.err, 2);
+    int it = 0;
+    for (int zi = 0; zi < nz && ok; ++zi) {
+      if (zi > 0) ok = mbar_wait(smem_u32(drained), (zi - 1) & 1, a.err, 4);
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t base = smem_u32(smem + s * STAGE);
-      const uint32_t bbase = base + ND * A_TILE;
-      // digit pairs (sa, o - sa) of order o into accumulator o
+      for (int i = 0; i < nk; ++i, ++it) {
+        const int s = it % ST;
+        ok = mbar_wait(smem_u32(&full[s]), (it / ST) & 1, a.err, 2);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t base = smem_u32(smem + s * STAGE);
+        const uint32_t bbase = base + ND * A_TILE;
+        // digit pairs (sa, o - sa) of order o into accumulator o
 #pragma unroll
-      for (int o = 0; o < ND; ++o) {
-        const uint32_t dcol = tmem + (uint32_t)o * ACC;
+        for (int o = 0; o < ND; ++o) {
+          const uint32_t dcol = tmem + (uint32_t)o * ACC;
 #pragma unroll
-        for (int sa = 0; sa <= o; ++sa) {
-          const uint64_t ad = kmajor_desc<BK>(base + sa * A_TILE);
-          const uint64_t bd = kmajor_desc<BK>(bbase + (o - sa) * B_TILE);
+          for (int sa = 0; sa <= o; ++sa) {
+            const uint64_t ad = kmajor_desc<BK>(base + sa * A_TILE);
+            const uint64_t bd = kmajor_desc<BK>(bbase + (o - sa) * B_TILE);
 #pragma unroll
-          for (int k = 0; k < KSTEPS; ++k)
-            umma_i8(dcol, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), IDESC,
-                    (i > 0 || sa > 0 || k > 0) ? 1u : 0u);
+            for (int k = 0; k < KSTEPS; ++k)
+              umma_i8(dcol, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), IDESC,
+                      (i > 0 || sa > 0 || k > 0) ? 1u : 0u);
+          }
+        }
+        umma_commit(smem_u32(&empty[s]));
+      }
+      // also after a failed wait: done then tracks the MMAs already issued,
+      // so tensor memory is not read or freed under them
+      umma_commit(smem_u32(done));
+    }
+  } else if (warp >= 2) {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+    const int q = warp & 3;
+    const int row = m0 + q * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+    for (int zi = 0; zi < nz && nk > 0; ++zi) {
+      const int z = z0 + zi;
+      bool have = false;
+      // bounded by time only: the MMAs must be finished before TMEM is read or freed
+      const uint64_t t0 = now_ns();
+      while (!(have = mbar_try(smem_u32(done), zi & 1))) {
+        if (now_ns() - t0 > kWaitNs) {
+          atomicCAS(a.err, 0, 3);
+          break;
+        }
+        __nanosleep(64);
+      }
+      have = have && *reinterpret_cast<volatile int*>(a.err) == 0;
+      have = __all_sync(0xffffffffu, have);   // tcgen05.ld is warp-collective
+      if (!have) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int bz = a.b_batched ? a.plane0 + z : 0;
+      const int era = row < a.M ? a.ea[(int64_t)(a.plane0 + z) * a.ea_stride + row] : 0;
+      double* orow = a.out + (int64_t)z * a.batch_stride_out + (int64_t)row * a.ld_out;
+      const int* ebz = a.eb + (int64_t)bz * a.eb_stride;
+      for (int c = 0; c < BN; c += 16) {
+        int v[ND][16];
+#pragma unroll
+        for (int o = 0; o < ND; ++o) tmem_ld16(trow + (uint32_t)o * ACC + c, v[o]);
+        if (row >= a.M) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + c + j;
+          if (col >= a.N) break;
+          // sum_o acc_o 2^-(14+8o), highest order first
+          double t = 0.0;
+#pragma unroll
+          for (int o = ND - 1; o >= 0; --o) t = t * 0x1p-8 + (double)v[o][j];
+          orow[col] = ldexp(t, era + ebz[col] - 14);
         }
       }
-      umma_commit(smem_u32(&bars[ST + s]));
-    }
-    // also after a failed wait: the done barrier then tracks the MMAs already
-    // issued, so tensor memory is not freed under them
-    umma_commit(smem_u32(&bars[2 * ST]));
-  }
-  __syncwarp();
-
-  bool have = false;
-  if (nk > 0) {
-    // bounded by time only: the MMAs must be finished before TMEM is freed
-    const uint64_t t0 = now_ns();
-    while (!(have = mbar_try(smem_u32(&bars[2 * ST]), 0))) {
-      if (now_ns() - t0 > kWaitNs) {
-        atomicCAS(a.err, 0, 3);
-        break;
-      }
-      __nanosleep(64);
-    }
-    have = have && *reinterpret_cast<volatile int*>(a.err) == 0;
-  }
-  have = __all_sync(0xffffffffu, have);   // tcgen05.ld is warp-collective
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (have) {
-    const int row = m0 + warp * 32 + lane;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    const int era = row < a.M ? a.ea[(int64_t)(a.plane0 + z) * a.ea_stride + row] : 0;
-    double* orow = a.out + (int64_t)z * a.batch_stride_out + (int64_t)row * a.ld_out;
-    const int* ebz = a.eb + (int64_t)bz * a.eb_stride;
-    for (int c = 0; c < BN; c += 16) {
-      int v[ND][16];
-#pragma unroll
-      for (int o = 0; o < ND; ++o) tmem_ld16(trow + (uint32_t)o * ACC + c, v[o]);
-      if (row >= a.M) continue;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int col = n0 + c + j;
-        if (col >= a.N) break;
-        // sum_o acc_o 2^-(14+8o), highest order first
-        double t = 0.0;
-#pragma unroll
-        for (int o = ND - 1; o >= 0; --o) t = t * 0x1p-8 + (double)v[o][j];
-        orow[col] = ldexp(t, era + ebz[col] - 14);
-      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(drained)) : "memory");
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -309,10 +333,13 @@ template <int ND, int BK, int BN, int ST>
 void launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
   constexpr size_t smem = smem_bytes<ND, BK, BN, ST>();
   static_assert(smem <= 232448, "stages exceed the shared memory of one CTA");
-  dim3 grid((a.N + BN - 1) / BN, (a.M + kBM - 1) / kBM, grid_z);
+  OzakiArgs b = a;
+  b.zcount = grid_z;
+  if (b.zper < 1) b.zper = 1;
+  dim3 grid((a.N + BN - 1) / BN, (a.M + kBM - 1) / kBM, (grid_z + b.zper - 1) / b.zper);
   DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8<ND, BK, BN, ST>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ozaki_gemm_i8<ND, BK, BN, ST><<<grid, 128, smem, s>>>(maps, a);
+  ozaki_gemm_i8<ND, BK, BN, ST><<<grid, 192, smem, s>>>(maps, b);
   DFJK_LAUNCHED();
 }
 

@@ -100,3 +100,34 @@ def test_mixed_is_deterministic():
     _, K1 = plan.jk(C)
     _, K2 = plan.jk(C)
     assert np.array_equal(K1.cpu().numpy(), K2.cpu().numpy())
+
+
+def test_mixed_chunked_build_is_bitwise_equal(water_golden):
+    """Digits depend only on their own row, so chunking the raw 3-center rows
+    (several int8 build GEMMs) changes nothing, bit for bit."""
+    from dftax_b200 import Plan
+
+    g = water_golden
+    orb, aux = golden_basis(g, "orb"), golden_basis(g, "aux")
+    a = Plan(orb, aux, precision="mixed").build()
+    b = Plan(orb, aux, precision="mixed", chunk_bytes=40_000).build()
+    Ja, Ka = a.jk(g["C"])
+    Jb, Kb = b.jk(g["C"])
+    assert np.array_equal(Ja.cpu().numpy(), Jb.cpu().numpy())
+    assert np.array_equal(Ka.cpu().numpy(), Kb.cpu().numpy())
+
+
+def test_mixed_screened_range_separated_vs_fp64():
+    """Screened pairs, the long-range fit and mixed precision together."""
+    from dftax_b200 import Plan, systems
+
+    sym, xyz, orb, aux, nocc = systems.workload("water8", seed=11)
+    p64 = Plan(orb, aux, screen=1e-9, omega=0.25).build()
+    pmx = Plan(orb, aux, screen=1e-9, omega=0.25, precision="mixed").build()
+    assert p64.long_range.info()["npair_shell"] == p64.info()["npair_shell"]
+    C = systems.random_occupied(p64.nao, nocc, seed=12)
+    P = 2.0 * C @ C.T
+    e64, F64 = p64.energy(P, 0.15, hf_coeff_lr=0.85)
+    emx, Fmx = pmx.energy(P, 0.15, hf_coeff_lr=0.85)
+    assert abs(emx - e64) < E_ABS
+    assert rel(Fmx[0].cpu().numpy(), F64[0].cpu().numpy()) < K_REL

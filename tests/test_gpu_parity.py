@@ -263,3 +263,33 @@ def test_errors_are_reported_not_trapped(water_golden):
     with pytest.raises(DfjkError) as ei:
         p.jk(g["C"])
     assert ei.value.status_name == "STATE"
+
+
+def test_fp64_k_is_bitwise_reproducible():
+    """The float64 X X^T sums its k slices in a fixed order."""
+    from dftax_b200 import Plan, systems
+
+    sym, xyz, orb, aux, nocc = systems.workload("water8", seed=4)
+    plan = Plan(orb, aux).build()
+    C = systems.random_occupied(plan.nao, nocc, seed=8)
+    _, K1 = plan.jk(C)
+    _, K2 = plan.jk(C)
+    K1 = K1.cpu().numpy()
+    assert np.array_equal(K1, K2.cpu().numpy())
+    assert np.array_equal(K1, K1.T)
+
+
+def test_trim_and_rebuild(water_golden):
+    """Cached device memory goes back to the driver; later plans still work."""
+    from dftax_b200 import Context, Plan
+
+    g = water_golden
+    orb, aux = golden_basis(g, "orb"), golden_basis(g, "aux")
+    a = Plan(orb, aux).build()
+    Ja, Ka = a.jk(g["C"])
+    a.close()
+    Context.get(0).trim()
+    b = Plan(orb, aux).build()
+    Jb, Kb = b.jk(g["C"])
+    assert np.array_equal(Ja.cpu().numpy(), Jb.cpu().numpy())
+    assert np.array_equal(Ka.cpu().numpy(), Kb.cpu().numpy())
