@@ -408,6 +408,12 @@ void launch_pair_setup(Plan& p, cudaStream_t s) {
 void launch_eri3c_rows(Plan& p, int64_t pair_begin, int64_t pair_end, int64_t row_base,
                        void* out, int64_t ld, bool f32, cudaStream_t s) {
   const Context& c = *p.ctx;
+  auto single = [](const std::vector<int>& np) {
+    for (int n : np)
+      if (n != 1) return false;
+    return true;
+  };
+  const int uncontracted = single(p.orb.nprim) && single(p.aux.nprim) ? 1 : 0;
   for (const ClassRange& cr : p.classes) {
     const int64_t b = pair_begin > cr.begin ? pair_begin : cr.begin;
     const int64_t e = pair_end < cr.begin + cr.count ? pair_end : cr.begin + cr.count;
@@ -436,6 +442,7 @@ void launch_eri3c_rows(Plan& p, int64_t pair_begin, int64_t pair_end, int64_t ro
       a.out = out;
       a.out_f32 = f32 ? 1 : 0;
       a.omega = p.atten;
+      a.uncontracted = uncontracted;
       const int ychunks = (a.aux_count + 127) / 128;
       for (int64_t q = b; q < e; q += (int64_t)1 << 30) {
         const int64_t n = (e - q) < ((int64_t)1 << 30) ? (e - q) : ((int64_t)1 << 30);

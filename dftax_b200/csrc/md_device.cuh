@@ -188,6 +188,7 @@ struct Eri3cArgs {
   void* out;
   int out_f32;               // 1: float output, 0: double
   double omega;              // > 0: erf(omega r)/r operator
+  int uncontracted;          // 1: every orbital and aux shell has one primitive
 };
 
 
