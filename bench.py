@@ -224,13 +224,24 @@ def fp64_gemm_peak(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def load_traffic(kernel: str, workload: str):
+def load_traffic(key: str, nrows: int, naux: int, ldb: int):
+    """DRAM bytes of the dominant kernel's launches in this step, scaled from
+    one ncu capture of a smaller workload (profiles/traffic.json) by its
+    measured-over-algorithmic ratio: the capture's traffic matched its
+    algorithmic bytes, and both grow with rows x row size."""
     p = os.path.join(HERE, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as fh:
-        d = json.load(fh)
-    return d.get(f"{kernel}@{workload}")
+        d = json.load(fh).get(key)
+    if d is None:
+        return None
+    naux16 = (naux + 15) // 16 * 16
+    alg = nrows * (5 * naux16 + 8 * ldb)
+    return {"bytes": round(d["ratio"] * alg), "algorithmic_bytes": alg,
+            "source": f"ncu capture of {d['kernel']} on {d['workload']}: dram read+write "
+                      f"{d['dram_bytes'] / 1e9:.3f} GB = {d['ratio']:.4f} x algorithmic; "
+                      f"scaled to this workload's rows and row size"}
 
 
 def int8_gemm_peak(torch):
@@ -403,7 +414,13 @@ def run_ours(args, rank, world, local_rank):
             "achieved": round(achieved, 3), "peak": round(peak, 3) if peak else None, "unit": unit,
             "frac": round(achieved / peak, 4) if peak else None, "peak_source": peak_src,
             "algorithmic": what, "ms_per_launch_group": round(phases[dom], 3),
-            "traffic": load_traffic(dom + ("@mixed" if mixed else ""), args.workload)}
+            "traffic": None}
+    tr = load_traffic("bgemm@mixed", nrows, naux, ldb) if mixed and dom == "bgemm" else None
+    if tr is not None:
+        # bytes of the phase's int8 GEMM launches (all raw-row chunks), like `achieved`
+        roof["traffic"] = tr["bytes"]
+        roof["traffic_algorithmic"] = tr["algorithmic_bytes"]
+        roof["traffic_source"] = tr["source"]
 
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,

@@ -131,3 +131,20 @@ def test_mixed_screened_range_separated_vs_fp64():
     emx, Fmx = pmx.energy(P, 0.15, hf_coeff_lr=0.85)
     assert abs(emx - e64) < E_ABS
     assert rel(Fmx[0].cpu().numpy(), F64[0].cpu().numpy()) < K_REL
+
+
+def test_mixed_open_shell_vs_fp64():
+    """Two spin channels: J of the total density, K per channel (terms.py:500-509)."""
+    from dftax_b200 import Plan, systems
+
+    sym, xyz, orb, aux, nocc = systems.workload("water3", seed=2)
+    p64, pmx = _pair(orb, aux)
+    n = p64.nao
+    Ca = systems.random_occupied(n, nocc, seed=3)
+    Cb = systems.random_occupied(n, nocc - 1, seed=4)
+    P = np.stack([Ca @ Ca.T, Cb @ Cb.T])
+    e64, F64 = p64.energy(P, 0.25)
+    emx, Fmx = pmx.energy(P, 0.25)
+    assert abs(emx - e64) < E_ABS
+    for s in range(2):
+        assert rel(Fmx[s].cpu().numpy(), F64[s].cpu().numpy()) < K_REL
