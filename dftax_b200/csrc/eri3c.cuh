@@ -16,6 +16,10 @@
 
 namespace dfjk {
 
+// classes up to this total angular momentum form R and W with compile-time
+// indices (hermite_r_ct, static_for): their arrays then stay in registers
+constexpr int kStaticM = 5;
+
 template <int LA, int LB, int LC>
 __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
   constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, NCC = nc_(LC);
@@ -48,7 +52,8 @@ __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
     double F[M + 1];
     boys_operator<M>(rho * (X * X + Y * Y + Z * Z), rho, a.omega, a.boys, a.boys_asym, F);
     double R[NR];
-    hermite_r<M>(rho, X, Y, Z, F, R);
+    if constexpr (M <= kStaticM) hermite_r_ct<M>(rho, X, Y, Z, F, R);
+    else hermite_r<M>(rho, X, Y, Z, F, R);
     double hob = 1.0;
     const double i2gc = -0.5 / gc;
 #pragma unroll
@@ -57,18 +62,32 @@ __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
 #pragma unroll 1
     for (int m = 0; m < NC; ++m) {
       double w[NH];
+      if constexpr (M <= kStaticM) {
+        // every R index a constant expression: R and w stay in registers
+        static_for<NH>([&](auto H) {
+          constexpr int h = decltype(H)::value, t = ht(h), u = hu(h), v = hv(h);
+          double s = 0.0;
+          static_for<NCC>([&](auto Cc) {
+            constexpr int c = decltype(Cc)::value;
+            constexpr int r = hidx(t + comp_x(LC, c), u + comp_y(LC, c), v + comp_z(LC, c));
+            s += sT[c * NC + m] * R[r];
+          });
+          w[h] = s * pref;
+        });
+      } else {
 #pragma unroll
-      for (int t = 0; t <= LAB; ++t)
+        for (int t = 0; t <= LAB; ++t)
 #pragma unroll
-        for (int u = 0; u <= LAB - t; ++u)
+          for (int u = 0; u <= LAB - t; ++u)
 #pragma unroll
-          for (int v = 0; v <= LAB - t - u; ++v) {
-            double s = 0.0;
+            for (int v = 0; v <= LAB - t - u; ++v) {
+              double s = 0.0;
 #pragma unroll
-            for (int c = 0; c < NCC; ++c)
-              s += sT[c * NC + m] * R[hidx(t + comp_x(LC, c), u + comp_y(LC, c), v + comp_z(LC, c))];
-            w[hidx(t, u, v)] = s * pref;
-          }
+              for (int c = 0; c < NCC; ++c)
+                s += sT[c * NC + m] * R[hidx(t + comp_x(LC, c), u + comp_y(LC, c), v + comp_z(LC, c))];
+              w[hidx(t, u, v)] = s * pref;
+            }
+      }
 #pragma unroll 1
       for (int i = 0; i < NAB; ++i) {
         const double* Ei = E + i * NH;

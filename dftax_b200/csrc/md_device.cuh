@@ -6,6 +6,9 @@
 
 #include "internal.h"
 
+#include <type_traits>
+#include <utility>
+
 namespace dfjk {
 
 // Hermite triples (t, u, v) with t + u + v <= L, packed by total order, then
@@ -29,6 +32,44 @@ __host__ __device__ constexpr int comp_y(int l, int k) {
 __host__ __device__ constexpr int comp_z(int l, int k) { return l - comp_x(l, k) - comp_y(l, k); }
 
 constexpr double kTwoPi25 = 34.98683665524972;   // 2 pi^{5/2}
+
+// (t, u, v) of the packed Hermite index h, at compile time (inverse of hidx)
+__host__ __device__ constexpr int horder(int h) {
+  int k = 0;
+  while (hcount(k) <= h) ++k;
+  return k;
+}
+__host__ __device__ constexpr int hsum_uv(int h) {
+  const int r = h - hcount(horder(h) - 1);
+  int q = 0;
+  while ((q + 1) * (q + 2) / 2 <= r) ++q;
+  return q;
+}
+__host__ __device__ constexpr int hv(int h) {
+  return h - hcount(horder(h) - 1) - hsum_uv(h) * (hsum_uv(h) + 1) / 2;
+}
+__host__ __device__ constexpr int hu(int h) { return hsum_uv(h) - hv(h); }
+__host__ __device__ constexpr int ht(int h) { return horder(h) - hsum_uv(h); }
+
+// f(std::integral_constant<int, i>) for i = 0 .. N-1 (or N-1 .. 0): every index
+// derived from i is a constant expression, so arrays indexed by it stay in
+// registers
+template <class F, int... I>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+template <int N, class F, int... I>
+__device__ __forceinline__ void static_for_desc_impl(F&& f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, N - 1 - I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for_desc(F&& f) {
+  static_for_desc_impl<N>(f, std::make_integer_sequence<int, N>{});
+}
 
 // Boys F_0..F_M at t: nearest table node + degree-6 Taylor for t < 40,
 // asymptotic 0.5 Gamma(n+1/2) t^{-n-1/2} beyond (dftax/energy/boys.py:130-176).
@@ -126,6 +167,45 @@ __device__ __forceinline__ void hermite_r(double rho, double X, double Y, double
     }
     R[0] = b[n];
   }
+}
+
+// hermite_r with every index a compile-time constant (for small M): the same
+// in-place ladder, entries visited in descending packed index (descending
+// order), so the orders k-1 and k-2 read still hold level m+1.
+template <int M>
+__device__ __forceinline__ void hermite_r_ct(double rho, double X, double Y, double Z,
+                                             const double (&F)[M + 1], double (&R)[hcount(M)]) {
+  double b[M + 1];
+  const double m2r = -2.0 * rho;
+  double pw = 1.0;
+#pragma unroll
+  for (int n = 0; n <= M; ++n) {
+    b[n] = pw * F[n];
+    pw *= m2r;
+  }
+  R[0] = b[M];
+  static_for<M>([&](auto L) {
+    constexpr int n = M - 1 - decltype(L)::value;
+    static_for_desc<hcount(M)>([&](auto H) {
+      constexpr int h = decltype(H)::value;
+      constexpr int k = horder(h), t = ht(h), u = hu(h), v = hv(h);
+      if constexpr (k >= 1 && k <= M - n) {
+        double val;
+        if constexpr (v > 0) {
+          val = Z * R[hidx(t, u, v - 1)];
+          if constexpr (v > 1) val += (v - 1) * R[hidx(t, u, v - 2)];
+        } else if constexpr (u > 0) {
+          val = Y * R[hidx(t, u - 1, 0)];
+          if constexpr (u > 1) val += (u - 1) * R[hidx(t, u - 2, 0)];
+        } else {
+          val = X * R[hidx(t - 1, 0, 0)];
+          if constexpr (t > 1) val += (t - 1) * R[hidx(t - 2, 0, 0)];
+        }
+        R[h] = val;
+      }
+    });
+    R[0] = b[n];
+  });
 }
 
 // Two-center E[i][j][t] for one axis, i <= LA, j <= LB, t <= i + j
