@@ -18,7 +18,7 @@ namespace dfjk {
 
 // classes up to this total angular momentum form R and W with compile-time
 // indices (hermite_r_ct, static_for): their arrays then stay in registers
-constexpr int kStaticM = 5;
+constexpr int kStaticM = 6;
 
 template <int LA, int LB, int LC>
 __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
 // The per-thread kernel above keeps each triple in one thread, whose R table
 // (up to 286 doubles) and accumulators then live in local memory.
 // ---------------------------------------------------------------------------
-constexpr int kCoopM = 6;
+constexpr int kCoopM = 7;
 
 template <int LA, int LB, int LC>
 struct CoopShape {
