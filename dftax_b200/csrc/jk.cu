@@ -1,4 +1,4 @@
-// J and K contractions over the fitted tensor B (float64 path).
+// J and K contractions over the fitted tensor B.
 //
 // B is row-major [nrows][ldb]: one row per AO pair (m, n) of a kept shell
 // pair, one column per kept metric direction (B = (mn|P) L, L L^T = V+).
@@ -7,7 +7,10 @@
 //      gamma   = B^T dvec                 (stream B once; CTA partials + reduce)
 //      J[m, n] = J[n, m] = B[r] . gamma   (stream B again; warp per row)
 //   K: X[m][x][i] = sum_{(r, n) in list(m)} B[r][x] C'[n][i]   (half transform)
-//      K = X X^T over the (x, i) index    (DSYRK), C' = C sqrt|w|
+//      K = X X^T over the (x, i) index, C' = C sqrt|w|
+// Float64 plans run both K products on the float64 tensor cores (mma.sync
+// m8n8k4 f64: the gathered half transform, then a split-k X X^T); mixed plans
+// run them on the int8 tensor cores (ozaki.cu). J is float64 in both.
 // which are the P-gradients of dftax's DFCoulomb.energy (terms.py:592-613):
 // J = int3c (V+ gamma), K = einsum("mlP,PQ,nsQ,ls->mn") (hybrid.py:23-41).
 #include "internal.h"
