@@ -293,3 +293,24 @@ def test_trim_and_rebuild(water_golden):
     Jb, Kb = b.jk(g["C"])
     assert np.array_equal(Ja.cpu().numpy(), Jb.cpu().numpy())
     assert np.array_equal(Ka.cpu().numpy(), Kb.cpu().numpy())
+
+
+def test_oversized_plan_reports_memory(water_golden):
+    """C40H82 unscreened in mixed precision needs ~136 GB for B plus ~136 GB of
+    digit planes, more than one B200 holds: the build reports MEMORY (after
+    emptying the device-memory cache and retrying), and the context stays
+    usable."""
+    from dftax_b200 import Context, Plan, systems
+    from dftax_b200._lib import DfjkError
+
+    sym, xyz, orb, aux, nocc = systems.workload("alkane40")
+    plan = Plan(orb, aux, precision="mixed")
+    with pytest.raises(DfjkError) as ei:
+        plan.build()
+    assert ei.value.status_name == "MEMORY"
+    plan.close()
+    Context.get(0).trim()
+    g = water_golden
+    small = Plan(golden_basis(g, "orb"), golden_basis(g, "aux")).build()
+    J, K = small.jk(g["C"])
+    assert rel(K.cpu().numpy(), g["K"]) < NOISE_REL
