@@ -348,7 +348,7 @@ void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int*
   const int64_t lplane = p.ldb * kp;
   for (int d = 0; d < ND; ++d)
     ozaki_map(&maps.b[d], p.ws_oz_l.as<int8_t>() + d * lplane, p.naux, p.ldb, 1, kp, lplane, bk,
-              sh.bn);
+              sh.box_b);
   OzakiArgs a{};
   a.N = (int)p.ldb;
   a.ktiles = (int)((p.naux + bk - 1) / bk);
@@ -358,10 +358,11 @@ void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int*
   a.ld_out = p.ldb;
   a.batch_stride_out = 0;
   a.err = p.ws_oz_err.as<int>();
-  // row blocks of at most 65535 * 128 rows (grid y)
-  const int64_t step = (int64_t)65535 * 128;
+  // row blocks of at most 65535 pairs of 128-row tiles (grid y)
+  const int64_t step = (int64_t)65535 * 256;
   for (int64_t m0 = 0; m0 < nr; m0 += step) {
     const int64_t mr = std::min(step, nr - m0);
+    ozaki_map_out(&maps.out, Bout + m0 * p.ldb, p.ldb, mr, p.ldb);
     for (int d = 0; d < ND; ++d)
       ozaki_map(&maps.a[d], planes + d * plane_stride + m0 * kp, p.naux, mr, 1, kp, plane_stride,
                 bk, 128);
@@ -395,7 +396,7 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
     ozaki_map(&maps.a[d], p.d_oz_a.as<int8_t>() + d * plane, nao, nao, p.nfit, nao_p, nao * nao_p,
               bk, 128);
     ozaki_map(&maps.b[d], p.ws_oz_c.as<int8_t>() + d * nsel * nao_p, nao, nsel, 1, nao_p,
-              nsel * nao_p, bk, sh.bn);
+              nsel * nao_p, bk, sh.box_b);
   }
   OzakiArgs a{};
   a.M = (int)nao;
@@ -448,7 +449,7 @@ void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, d
   for (int d = 0; d < ND; ++d) {
     const int8_t* base = p.ws_oz_x.as<int8_t>() + d * plane;
     ozaki_map(&maps.a[d], base, KS, nao, nsl, KS, nao * KS, bk, 128);
-    ozaki_map(&maps.b[d], base, KS, nao, nsl, KS, nao * KS, bk, sh.bn);
+    ozaki_map(&maps.b[d], base, KS, nao, nsl, KS, nao * KS, bk, sh.box_b);
   }
   OzakiArgs a{};
   a.M = (int)nao;

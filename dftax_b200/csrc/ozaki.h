@@ -20,12 +20,14 @@ constexpr int64_t kOzSlice = 8192;  // k bytes per slice of the K = X X^T produc
 enum OzakiShape { kOzBuild = 0, kOzHalf = 1, kOzSyrk = 2 };
 struct OzakiShapeInfo {
   int digits, box_k, bn, stages;   // digits per value, k tile bytes, n tile, ring depth
+  int box_b;                       // B rows per copy: bn, or bn / 2 on SM pairs
 };
 OzakiShapeInfo ozaki_shape(OzakiShape shape);
 
 struct OzakiMaps {
   CUtensorMap a[kOzMaxDigits];   // A digit planes, box (box_k, 128 rows, 1)
-  CUtensorMap b[kOzMaxDigits];   // B digit planes, box (box_k, bn rows, 1)
+  CUtensorMap b[kOzMaxDigits];   // B digit planes, box (box_k, box_b rows, 1)
+  CUtensorMap out;               // build product: float64 output, box (16, 32), 128-byte swizzle
 };
 
 struct OzakiArgs {
@@ -49,7 +51,11 @@ struct OzakiArgs {
 void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
                int64_t stride1, int64_t stride2, int box_k, int box1);
 
-// grid (ceil(N/bn), ceil(M/128), ceil(nbatch / a.zper)): nbatch batches (grid_z)
+// float64 output map of the build product over [rows][cols] (ld elements per row)
+void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t rows, int64_t ld);
+
+// grid (ceil(N/bn), ceil(M/128), ceil(nbatch / a.zper)): nbatch batches (grid_z);
+// the build product: clusters of two CTAs, grid (2 ceil(N/bn), ceil(M/256)), one batch
 void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, int grid_z,
                   cudaStream_t s);
 

@@ -7,7 +7,8 @@
 // s times digit t weighs 2^-(14+8(s+t)), so the ND(ND+1)/2 products of
 // combined order o = s + t < ND are accumulated EXACTLY in int32 (kind::i8
 // MMA), one tensor-memory accumulator per order, and the epilogue combines
-// them in float64 with weights 2^-(14+8o). Exactness needs k * (sum over an
+// them exactly in int64 with weights 2^-(14+8o) before one rounding to
+// float64. Exactness needs k * (sum over an
 // order of |d_s d_t|) < 2^31: k <= kOzMaxK. The only error is the truncation
 // of the digit expansion (2^-(8 ND) of 2^e, at most 2^(2-8ND) of the row
 // maximum); unlike fp32 accumulation there is no rounding drift with k. (Float32 accumulation of split-bf16 products was
@@ -18,8 +19,9 @@
 // BK-byte swizzle into an ST-stage mbarrier ring (ND digit planes per operand
 // per stage). Two shapes are compiled: ND 4, BK 128, BN 80, two 104 KB stages
 // (K half transform: n = occupied orbitals, 160 = 2 x 80 for (H2O)_32), and
-// ND 5, BK 64, BN 96, three 70 KB stages (build product and K = X X^T;
-// 5 x 96 of the 512 TMEM columns). Warp 0 lane 0 issues
+// ND 5, BK 64, BN 96, three 70 KB stages (K = X X^T; 5 x 96 of the 512 TMEM
+// columns). The build product runs on SM pairs (ozaki_gemm_i8_pair below,
+// M = 256, four 55 KB stages). Warp 0 lane 0 issues
 // copies, warp 1 lane 0 issues MMAs (BK/32 per digit pair per k tile), all
 // four warps drain tensor memory (warp w owns rows 32w..32w+31). Every wait
 // is bounded (4 s of %globaltimer); a timeout sets *err, skips the remaining
@@ -121,8 +123,7 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v) {
-  uint32_t r[16];
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t* r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
       "%12, %13, %14, %15}, [%16];"
@@ -130,9 +131,39 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int* v) {
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
         "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// keeps every use of r after the preceding tcgen05.wait::ld
+__device__ __forceinline__ void reg_fence16(uint32_t* r) {
+  asm volatile(""
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
+}
+
+// sum_o acc_o 2^-(14+8o) 2^e: the orders combine exactly in int64 (order 0
+// is below 2^28 and order 1 below 2^30 for k <= kOzMaxK, so the sum stays
+// below 2^60) and round once to float64; 5 int-to-float64 conversions and 4
+// float64 FMAs per value made the epilogue the slowest part of a tile
+template <int ND>
+__device__ __forceinline__ double combine_orders(const uint32_t (&v)[ND][16], int j, int e) {
+  long long s = (int)v[0][j];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = (int)r[i];
+  for (int o = 1; o < ND; ++o) s = s * 256 + (int)v[o][j];
+  return ldexp((double)s, e - 14 - 8 * (ND - 1));
+}
+
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t src, int c0, int c1) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(src), "r"(c0), "r"(c1)
+               : "memory");
 }
 
 template <int ND, int BK, int BN, int ST>
@@ -277,19 +308,18 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
       double* orow = a.out + (int64_t)z * a.batch_stride_out + (int64_t)row * a.ld_out;
       const int* ebz = a.eb + (int64_t)bz * a.eb_stride;
       for (int c = 0; c < BN; c += 16) {
-        int v[ND][16];
+        uint32_t v[ND][16];
 #pragma unroll
-        for (int o = 0; o < ND; ++o) tmem_ld16(trow + (uint32_t)o * ACC + c, v[o]);
+        for (int o = 0; o < ND; ++o) tmem_ld16_issue(trow + (uint32_t)o * ACC + c, v[o]);
+        tmem_ld_wait();
+#pragma unroll
+        for (int o = 0; o < ND; ++o) reg_fence16(v[o]);
         if (row >= a.M) continue;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int col = n0 + c + j;
           if (col >= a.N) break;
-          // sum_o acc_o 2^-(14+8o), highest order first
-          double t = 0.0;
-#pragma unroll
-          for (int o = ND - 1; o >= 0; --o) t = t * 0x1p-8 + (double)v[o][j];
-          orow[col] = ldexp(t, era + ebz[col] - 14);
+          orow[col] = combine_orders<ND>(v, j, era + ebz[col]);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -301,6 +331,245 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                 : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Two-SM form of the same product (tcgen05 cta_group::2, M = 256) for the
+// build product B = (ij|P) L. A cluster of two CTAs (consecutive in x, so a
+// pair and the n tiles after it share A rows in L2) shares an n tile: each CTA
+// loads its own 128 rows of A and half of the BN rows of B, the leader (rank 0)
+// issues the MMAs, which read A from each CTA's shared memory and B from both
+// halves, and each CTA's TMEM receives its 128 rows x BN columns. Per MMA a
+// CTA thus reads (128 + BN/2) * 32 bytes of operands instead of
+// (128 + BN) * 32, and its TMA writes (128 + BN/2) * BK bytes per digit and k
+// tile instead of (128 + BN) * BK: shared-memory bandwidth, not the tensor
+// pipe, bounds the one-SM kernel at BN = 96, and TMEM (5 orders x BN of 512
+// columns) caps BN.
+//   * both CTAs' TMA loads complete on the leader's full barrier (its cluster
+//     address from mapa; cta_group::2 form of the tiled copy);
+//   * the leader's commits arrive on both CTAs' empty / done barriers
+//     (tcgen05.commit multicast);
+//   * TMEM is allocated and freed cta_group::2 by warp 0 of each CTA;
+//   * cluster barriers after the setup and before the teardown keep the peer's
+//     shared memory alive while the leader's MMAs may still read it.
+//   * eight epilogue warps (two per TMEM lane quarter, half the columns each)
+//     combine the orders and stage 32 x 16 float64 blocks in the idle stage
+//     memory for TMA tensor stores.
+// Every mbarrier wait is bounded as in the one-SM kernel.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t leader_addr(uint32_t cta_addr) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, 0;" : "=r"(r) : "r"(cta_addr));
+  return r;
+}
+
+__device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap* map,
+                                                 uint32_t leader_mbar, int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(leader_mbar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                             uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit_pair(uint32_t mbar) {
+  const uint16_t both = 0x3;
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(mbar),
+      "h"(both)
+      : "memory");
+}
+
+template <int ND, int BK, int BN, int ST>
+__global__ void __launch_bounds__(320, 1) ozaki_gemm_i8_pair(const __grid_constant__ OzakiMaps maps,
+                                                             OzakiArgs a) {
+  constexpr int BH = BN / 2;                 // B rows loaded by each CTA
+  constexpr uint32_t A_TILE = kBM * BK;
+  constexpr uint32_t B_TILE = BH * BK;
+  constexpr uint32_t STAGE = ND * (A_TILE + B_TILE);
+  constexpr int KSTEPS = BK / 32;
+  constexpr uint32_t ACC = (ND * 128 <= (int)kTmemCols) ? 128 : BN;
+  constexpr uint32_t STG = 32 * 128;         // one warp's 32 x 16 float64 block
+  static_assert(ND * ACC <= kTmemCols, "order accumulators exceed tensor memory");
+  static_assert(A_TILE % 1024 == 0 && B_TILE % 1024 == 0, "tiles must keep 1 KB alignment");
+  static_assert(BN % 32 == 0, "two-SM i8 MMA needs N a multiple of 32");
+  static_assert((BN / 2) % 16 == 0, "each epilogue warp takes whole 16-column chunks");
+  static_assert(4 * (BN / 16) * STG <= ST * STAGE, "output staging exceeds the stage memory");
+  // S32 accumulator, signed int8 A and B, N>>3, M = 256 >> 4
+  constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                             ((uint32_t)(256 >> 4) << 24);
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * STAGE);
+  uint64_t* empty = full + ST;
+  uint64_t* done = empty + ST;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  int* ebs = reinterpret_cast<int*>(tmem_slot + 4);   // exponents of the n tile's columns
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  // blockIdx.x = 2 * (n tile) + rank, blockIdx.y = pair of m tiles
+  const int n0 = (blockIdx.x >> 1) * BN, m0 = (blockIdx.y * 2 + (int)rank) * kBM;
+  const int nk = a.ktiles;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    mbar_init(smem_u32(done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  cluster_sync();   // both CTAs' barriers exist before any load or commit targets them
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (threadIdx.x == 0 && nk > 0) {
+    // producer of this CTA: its A rows and its half of B, counted on the leader's barrier
+    int issued = 0;
+    bool ok = true;
+    for (int i = 0; i < nk; ++i, ++issued) {
+      const int s = i % ST;
+      if (i >= ST) ok = mbar_wait(smem_u32(&empty[s]), ((i / ST) - 1) & 1, a.err, 1);
+      if (!ok) break;
+      const uint32_t fb = leader_addr(smem_u32(&full[s]));
+      if (leader) mbar_expect_tx(smem_u32(&full[s]), 2 * STAGE);
+      uint8_t* st = smem + s * STAGE;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        tma_load_3d_pair(smem_u32(st + d * A_TILE), &maps.a[d], fb, i * BK, m0, a.plane0);
+        tma_load_3d_pair(smem_u32(st + ND * A_TILE + d * B_TILE), &maps.b[d], fb, i * BK,
+                         n0 + (int)rank * BH, 0);
+      }
+    }
+    if (!ok && leader) {
+      // the copies in flight complete on the leader's barriers (bounded)
+      for (int q = issued - ST > 0 ? issued - ST : 0; q < issued; ++q) {
+        const uint64_t t0 = now_ns();
+        while (!mbar_try(smem_u32(&full[q % ST]), (q / ST) & 1) && now_ns() - t0 < kWaitNs)
+          __nanosleep(64);
+      }
+    }
+  } else if (threadIdx.x == 32 && nk > 0 && leader) {
+    bool ok = true;
+    for (int i = 0; i < nk; ++i) {
+      const int s = i % ST;
+      ok = mbar_wait(smem_u32(&full[s]), (i / ST) & 1, a.err, 2);
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t base = smem_u32(smem + s * STAGE);
+      const uint32_t bbase = base + ND * A_TILE;
+#pragma unroll
+      for (int o = 0; o < ND; ++o) {
+        const uint32_t dcol = tmem + (uint32_t)o * ACC;
+#pragma unroll
+        for (int sa = 0; sa <= o; ++sa) {
+          const uint64_t ad = kmajor_desc<BK>(base + sa * A_TILE);
+          const uint64_t bd = kmajor_desc<BK>(bbase + (o - sa) * B_TILE);
+#pragma unroll
+          for (int k = 0; k < KSTEPS; ++k)
+            umma_i8_pair(dcol, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), IDESC,
+                         (i > 0 || sa > 0 || k > 0) ? 1u : 0u);
+        }
+      }
+      umma_commit_pair(smem_u32(&empty[s]));
+    }
+    // also after a failed wait: done then tracks the MMAs already issued
+    umma_commit_pair(smem_u32(done));
+  } else if (warp >= 2 && nk > 0) {
+    // epilogue, eight warps: warp w reads TMEM lanes 32 (w % 4) .. + 31 of this
+    // CTA (rows row0 .. row0 + 31) and columns h BN/2 .. of them, h = (w - 2) / 4,
+    // and stores them through shared memory with TMA
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    const int row0 = m0 + q * 32, row = row0 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+    for (int j = threadIdx.x - 64; j < BN; j += 256) ebs[j] = n0 + j < a.N ? a.eb[n0 + j] : 0;
+    asm volatile("bar.sync 1, 256;" ::: "memory");   // the eight epilogue warps
+    bool have = false;
+    const uint64_t t0 = now_ns();
+    while (!(have = mbar_try(smem_u32(done), 0))) {
+      if (now_ns() - t0 > kWaitNs) {
+        atomicCAS(a.err, 0, 3);
+        break;
+      }
+      __nanosleep(64);
+    }
+    have = have && *reinterpret_cast<volatile int*>(a.err) == 0;
+    have = __all_sync(0xffffffffu, have);   // tcgen05.ld is warp-collective
+    if (have) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int era = row < a.M ? a.ea[row] : 0;
+      // the stage memory is idle once done has fired: every copy landed and
+      // every MMA that read it (in either CTA) has completed
+      uint8_t* stg = smem + (uint32_t)q * (BN / 16) * STG;
+      for (int c = h * (BN / 2); c < (h + 1) * (BN / 2); c += 16) {
+        uint32_t v[ND][16];
+#pragma unroll
+        for (int o = 0; o < ND; ++o) tmem_ld16_issue(trow + (uint32_t)o * ACC + c, v[o]);
+        tmem_ld_wait();
+#pragma unroll
+        for (int o = 0; o < ND; ++o) reg_fence16(v[o]);
+        // this lane's 128-byte row of the block, 16-byte chunks in the
+        // 128-byte swizzle of the output tensor map (chunk j at j ^ (row % 8))
+        uint8_t* buf = stg + (uint32_t)(c / 16) * STG + lane * 128;
+#pragma unroll
+        for (int j = 0; j < 16; j += 2) {
+          const double r0 = combine_orders<ND>(v, j, era + ebs[c + j]);
+          const double r1 = combine_orders<ND>(v, j + 1, era + ebs[c + j + 1]);
+          *reinterpret_cast<double2*>(buf + (((j >> 1) ^ (lane & 7)) << 4)) = make_double2(r0, r1);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+          // rows past M and columns past N are clipped by the tensor map
+          tma_store_2d(&maps.out, smem_u32(stg + (uint32_t)(c / 16) * STG), n0 + c, row0);
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+      }
+      if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      __syncwarp();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  cluster_sync();   // the leader's MMAs are done before either CTA frees or leaves
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
                  : "memory");
 }
 
@@ -343,14 +612,49 @@ void launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t 
   DFJK_LAUNCHED();
 }
 
+template <int ND, int BK, int BN, int ST>
+constexpr size_t smem_bytes_pair() {
+  return (size_t)ST * ND * (kBM * BK + (BN / 2) * BK) + 1024 + 128 + 4 * BN;
+}
+
+// clusters of two CTAs along x: grid (2 * ceil(N/BN), ceil(M/256)), one batch
+template <int ND, int BK, int BN, int ST>
+void launch_pair(const OzakiMaps& maps, const OzakiArgs& a, cudaStream_t s) {
+  constexpr size_t smem = smem_bytes_pair<ND, BK, BN, ST>();
+  static_assert(smem <= 232448, "stages exceed the shared memory of one CTA");
+  OzakiArgs b = a;
+  b.zcount = 1;
+  b.zper = 1;
+  const int mpairs = (a.M + 2 * kBM - 1) / (2 * kBM);
+  if (mpairs > 65535) fail(DFJK_ERR_INVALID, "two-SM int8 GEMM: too many row tiles");
+  auto* kern = ozaki_gemm_i8_pair<ND, BK, BN, ST>;
+  DFJK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * ((a.N + BN - 1) / BN), mpairs, 1);
+  cfg.blockDim = dim3(320, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  DFJK_CUDA(cudaLaunchKernelEx(&cfg, kern, maps, b));
+  DFJK_LAUNCHED();
+}
+
 }  // namespace
 
-// digits, k tile bytes, n tile, stages of each product (see ozaki.h)
+// digits, k tile bytes, n tile, stages and B rows per copy of each product
+// (see ozaki.h); the build product runs on SM pairs, each CTA copying half of
+// the n tile
 OzakiShapeInfo ozaki_shape(OzakiShape shape) {
   switch (shape) {
-    case kOzHalf: return {kOzKDigits, 128, 80, 2};
-    case kOzBuild: return {kOzBDigits, 64, 96, 3};
-    case kOzSyrk: return {kOzSDigits, 64, 96, 3};
+    case kOzHalf: return {kOzKDigits, 128, 80, 2, 80};
+    case kOzBuild: return {kOzBDigits, 64, 96, 4, 48};
+    case kOzSyrk: return {kOzSDigits, 64, 96, 3, 96};
   }
   fail(DFJK_ERR_INVALID, "unknown int8 GEMM shape %d", (int)shape);
 }
@@ -371,6 +675,19 @@ void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t
   if (r != CUDA_SUCCESS) fail(DFJK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
 
+void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t rows, int64_t ld) {
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 8) % 16))
+    fail(DFJK_ERR_INVALID, "output tensor map: base or row pitch not 16-byte aligned");
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * 8)};
+  cuuint32_t box[2] = {16, 32};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(DFJK_ERR_CUDA, "cuTensorMapEncodeTiled (output) failed (%d)", (int)r);
+}
+
 void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, int grid_z,
                   cudaStream_t s) {
   if (grid_z <= 0 || a.M <= 0 || a.N <= 0) return;
@@ -379,6 +696,9 @@ void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, i
   switch (shape) {
     case kOzHalf: launch<4, 128, 80, 2>(maps, a, grid_z, s); return;
     case kOzBuild:
+      if (grid_z != 1) fail(DFJK_ERR_INVALID, "the two-SM build product takes one batch");
+      launch_pair<5, 64, 96, 4>(maps, a, s);
+      return;
     case kOzSyrk: launch<5, 64, 96, 3>(maps, a, grid_z, s); return;
   }
   fail(DFJK_ERR_INVALID, "unknown int8 GEMM shape %d", (int)shape);
