@@ -362,7 +362,7 @@ void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int*
   const int64_t step = (int64_t)65535 * 256;
   for (int64_t m0 = 0; m0 < nr; m0 += step) {
     const int64_t mr = std::min(step, nr - m0);
-    ozaki_map_out(&maps.out, Bout + m0 * p.ldb, p.ldb, mr, p.ldb);
+    ozaki_map_out(&maps.out, Bout + m0 * p.ldb, p.ldb, 1, mr, p.ldb, p.ldb);
     for (int d = 0; d < ND; ++d)
       ozaki_map(&maps.a[d], planes + d * plane_stride + m0 * kp, p.naux, mr, 1, kp, plane_stride,
                 bk, 128);
@@ -420,6 +420,9 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
     const int64_t nz = std::min<int64_t>(zstep, n - z0);
     a.plane0 = (int)(x0 + z0);
     a.out = X + z0 * nsel;
+    // X[m][z][i] leaves through TMA tensor stores when its strides allow
+    a.tma_out = ozaki_out_mappable(a.out, a.batch_stride_out, a.ld_out) ? 1 : 0;
+    if (a.tma_out) ozaki_map_out(&maps.out, a.out, nsel, nz, nao, a.batch_stride_out, a.ld_out);
     ozaki_launch(kOzHalf, maps, a, (int)nz, s);
   }
   check_oz_err(p, s);

@@ -27,7 +27,7 @@ OzakiShapeInfo ozaki_shape(OzakiShape shape);
 struct OzakiMaps {
   CUtensorMap a[kOzMaxDigits];   // A digit planes, box (box_k, 128 rows, 1)
   CUtensorMap b[kOzMaxDigits];   // B digit planes, box (box_k, box_b rows, 1)
-  CUtensorMap out;               // build product: float64 output, box (16, 32), 128-byte swizzle
+  CUtensorMap out;               // float64 output when tma_out: box (16, 1, 32), 128-byte swizzle
 };
 
 struct OzakiArgs {
@@ -44,6 +44,7 @@ struct OzakiArgs {
   int* err;                // set non-zero when a bounded wait gives up
   int zper;                // batches per CTA (one TMEM allocation, one ring); 0 or 1: one
   int zcount;              // batches of the launch (set by ozaki_launch)
+  int tma_out;             // half transform: 1 writes through maps.out (the build product always does)
 };
 
 // 3-D int8 tensor map over [d2][d1][d0] (d0 contiguous; strides in bytes),
@@ -51,8 +52,11 @@ struct OzakiArgs {
 void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t d2,
                int64_t stride1, int64_t stride2, int box_k, int box1);
 
-// float64 output map of the build product over [rows][cols] (ld elements per row)
-void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t rows, int64_t ld);
+// float64 output map over [rows][batches][cols] (strides in elements), and
+// whether a base and strides allow one (16-byte alignment)
+bool ozaki_out_mappable(const double* base, int64_t batch_stride, int64_t ld);
+void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t batches, int64_t rows,
+                   int64_t batch_stride, int64_t ld);
 
 // grid (ceil(N/bn), ceil(M/128), ceil(nbatch / a.zper)): nbatch batches (grid_z);
 // the build product: clusters of two CTAs, grid (2 ceil(N/bn), ceil(M/256)), one batch

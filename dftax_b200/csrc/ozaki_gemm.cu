@@ -151,22 +151,45 @@ __device__ __forceinline__ void reg_fence16(uint32_t* r) {
 // is below 2^28 and order 1 below 2^30 for k <= kOzMaxK, so the sum stays
 // below 2^60) and round once to float64; 5 int-to-float64 conversions and 4
 // float64 FMAs per value made the epilogue the slowest part of a tile
+// x 2^e: a multiply by the power of two while 2^e is a normal double (the
+// product rounds as ldexp's result does), ldexp beyond; ldexp itself per
+// value cost more than the rest of the epilogue arithmetic
+__device__ __forceinline__ double scale_pow2(double x, int e) {
+  if (e >= -1022 && e <= 1023) return x * __longlong_as_double((long long)(e + 1023) << 52);
+  return ldexp(x, e);
+}
+
 template <int ND>
 __device__ __forceinline__ double combine_orders(const uint32_t (&v)[ND][16], int j, int e) {
   long long s = (int)v[0][j];
 #pragma unroll
   for (int o = 1; o < ND; ++o) s = s * 256 + (int)v[o][j];
-  return ldexp((double)s, e - 14 - 8 * (ND - 1));
+  return scale_pow2((double)s, e - 14 - 8 * (ND - 1));
 }
 
-__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t src, int c0, int c1) {
-  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int c0, int c1,
+                                             int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
                    reinterpret_cast<uint64_t>(map)),
-               "r"(src), "r"(c0), "r"(c1)
+               "r"(src), "r"(c0), "r"(c1), "r"(c2)
                : "memory");
 }
 
-template <int ND, int BK, int BN, int ST>
+// one lane's 128-byte row of a 32 x 16 float64 block in shared memory, in the
+// 128-byte swizzle of the output tensor maps (16-byte chunk j at j ^ (row % 8))
+template <int ND>
+__device__ __forceinline__ void stage_row(uint8_t* buf, int lane, const uint32_t (&v)[ND][16],
+                                          int era, const int* ecol) {
+#pragma unroll
+  for (int j = 0; j < 16; j += 2) {
+    const double r0 = combine_orders<ND>(v, j, era + ecol[j]);
+    const double r1 = combine_orders<ND>(v, j + 1, era + ecol[j + 1]);
+    *reinterpret_cast<double2*>(buf + lane * 128 + (((j >> 1) ^ (lane & 7)) << 4)) =
+        make_double2(r0, r1);
+  }
+}
+
+template <int ND, int BK, int BN, int ST, bool TOUT>
 __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ OzakiMaps maps,
                                                         OzakiArgs a) {
   constexpr uint32_t A_TILE = kBM * BK;
@@ -183,9 +206,13 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
-  // barriers: full[ST], empty[ST], done (accumulators of a batch final),
-  // drained (the epilogue warps have read them)
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * STAGE);
+  // TOUT: per epilogue warp two 32 x 16 float64 staging blocks after the ring
+  // (outputs leave through maps.out); barriers: full[ST], empty[ST], done
+  // (accumulators of a batch final), drained (the epilogue warps have read them)
+  constexpr uint32_t STG_BYTES = TOUT ? 4 * 2 * 4096 : 0;
+  static_assert(BN % 16 == 0, "16-column epilogue chunks");
+  uint8_t* stg = smem + ST * STAGE;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * STAGE + STG_BYTES);
   uint64_t* empty = full + ST;
   uint64_t* done = empty + ST;
   uint64_t* drained = done + 1;
@@ -285,8 +312,9 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
   } else if (warp >= 2) {
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
     const int q = warp & 3;
-    const int row = m0 + q * 32 + lane;
+    const int row0 = m0 + q * 32, row = row0 + lane;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+    int nst = 0;   // TOUT: blocks this warp has handed to TMA (double buffer index)
     for (int zi = 0; zi < nz && nk > 0; ++zi) {
       const int z = z0 + zi;
       bool have = false;
@@ -314,18 +342,39 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
         tmem_ld_wait();
 #pragma unroll
         for (int o = 0; o < ND; ++o) reg_fence16(v[o]);
-        if (row >= a.M) continue;
+        if constexpr (TOUT) {
+          // columns past N read exponent 0; the tensor map clips them and rows past M
+          int ecol[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c + j;
-          if (col >= a.N) break;
-          orow[col] = combine_orders<ND>(v, j, era + ebz[col]);
+          for (int j = 0; j < 16; ++j) ecol[j] = n0 + c + j < a.N ? ebz[n0 + c + j] : 0;
+          uint8_t* buf = stg + (uint32_t)(q * 2 + (nst & 1)) * 4096;
+          // the block handed over two chunks ago has been read out of this buffer
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+          __syncwarp();
+          stage_row<ND>(buf, lane, v, era, ecol);
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_3d(&maps.out, smem_u32(buf), n0 + c, z, row0);
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          }
+          ++nst;
+        } else {
+          if (row >= a.M) continue;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c + j;
+            if (col >= a.N) break;
+            orow[col] = combine_orders<ND>(v, j, era + ebz[col]);
+          }
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(drained)) : "memory");
     }
+    // the staging blocks must be read out before the CTA's shared memory goes
+    if (TOUT && lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -544,20 +593,13 @@ __global__ void __launch_bounds__(320, 1) ozaki_gemm_i8_pair(const __grid_consta
         tmem_ld_wait();
 #pragma unroll
         for (int o = 0; o < ND; ++o) reg_fence16(v[o]);
-        // this lane's 128-byte row of the block, 16-byte chunks in the
-        // 128-byte swizzle of the output tensor map (chunk j at j ^ (row % 8))
-        uint8_t* buf = stg + (uint32_t)(c / 16) * STG + lane * 128;
-#pragma unroll
-        for (int j = 0; j < 16; j += 2) {
-          const double r0 = combine_orders<ND>(v, j, era + ebs[c + j]);
-          const double r1 = combine_orders<ND>(v, j + 1, era + ebs[c + j + 1]);
-          *reinterpret_cast<double2*>(buf + (((j >> 1) ^ (lane & 7)) << 4)) = make_double2(r0, r1);
-        }
+        uint8_t* buf = stg + (uint32_t)(c / 16) * STG;
+        stage_row<ND>(buf, lane, v, era, ebs + c);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
         if (lane == 0) {
           // rows past M and columns past N are clipped by the tensor map
-          tma_store_2d(&maps.out, smem_u32(stg + (uint32_t)(c / 16) * STG), n0 + c, row0);
+          tma_store_3d(&maps.out, smem_u32(buf), n0 + c, 0, row0);
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
       }
@@ -593,22 +635,22 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-template <int ND, int BK, int BN, int ST>
+template <int ND, int BK, int BN, int ST, bool TOUT>
 constexpr size_t smem_bytes() {
-  return (size_t)ST * ND * (kBM * BK + BN * BK) + 1024 + 256;
+  return (size_t)ST * ND * (kBM * BK + BN * BK) + (TOUT ? 4 * 2 * 4096 : 0) + 1024 + 256;
 }
 
-template <int ND, int BK, int BN, int ST>
+template <int ND, int BK, int BN, int ST, bool TOUT>
 void launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t s) {
-  constexpr size_t smem = smem_bytes<ND, BK, BN, ST>();
+  constexpr size_t smem = smem_bytes<ND, BK, BN, ST, TOUT>();
   static_assert(smem <= 232448, "stages exceed the shared memory of one CTA");
   OzakiArgs b = a;
   b.zcount = grid_z;
   if (b.zper < 1) b.zper = 1;
   dim3 grid((a.N + BN - 1) / BN, (a.M + kBM - 1) / kBM, (grid_z + b.zper - 1) / b.zper);
-  DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8<ND, BK, BN, ST>,
+  DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8<ND, BK, BN, ST, TOUT>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ozaki_gemm_i8<ND, BK, BN, ST><<<grid, 192, smem, s>>>(maps, b);
+  ozaki_gemm_i8<ND, BK, BN, ST, TOUT><<<grid, 192, smem, s>>>(maps, b);
   DFJK_LAUNCHED();
 }
 
@@ -652,7 +694,7 @@ void launch_pair(const OzakiMaps& maps, const OzakiArgs& a, cudaStream_t s) {
 // the n tile
 OzakiShapeInfo ozaki_shape(OzakiShape shape) {
   switch (shape) {
-    case kOzHalf: return {kOzKDigits, 128, 80, 2, 80};
+    case kOzHalf: return {kOzKDigits, 64, 80, 3, 80};
     case kOzBuild: return {kOzBDigits, 64, 96, 4, 48};
     case kOzSyrk: return {kOzSDigits, 64, 96, 3, 96};
   }
@@ -675,14 +717,20 @@ void ozaki_map(CUtensorMap* m, const void* base, int64_t d0, int64_t d1, int64_t
   if (r != CUDA_SUCCESS) fail(DFJK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
 
-void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t rows, int64_t ld) {
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * 8) % 16))
-    fail(DFJK_ERR_INVALID, "output tensor map: base or row pitch not 16-byte aligned");
-  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)(ld * 8)};
-  cuuint32_t box[2] = {16, 32};
-  cuuint32_t es[2] = {1, 1};
-  CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, es,
+bool ozaki_out_mappable(const double* base, int64_t batch_stride, int64_t ld) {
+  return !(reinterpret_cast<uintptr_t>(base) & 15) && (batch_stride * 8) % 16 == 0 &&
+         (ld * 8) % 16 == 0;
+}
+
+void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t batches, int64_t rows,
+                   int64_t batch_stride, int64_t ld) {
+  if (!ozaki_out_mappable(base, batch_stride, ld))
+    fail(DFJK_ERR_INVALID, "output tensor map: base or strides not 16-byte aligned");
+  cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)batches, (cuuint64_t)rows};
+  cuuint64_t strides[2] = {(cuuint64_t)(batch_stride * 8), (cuuint64_t)(ld * 8)};
+  cuuint32_t box[3] = {16, 1, 32};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, es,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) fail(DFJK_ERR_CUDA, "cuTensorMapEncodeTiled (output) failed (%d)", (int)r);
@@ -694,12 +742,15 @@ void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, i
   static_assert(kOzKDigits == 4 && kOzBDigits == 5 && kOzSDigits == 5,
                 "the compiled shapes follow the digit counts");
   switch (shape) {
-    case kOzHalf: launch<4, 128, 80, 2>(maps, a, grid_z, s); return;
+    case kOzHalf:
+      if (a.tma_out) launch<4, 64, 80, 3, true>(maps, a, grid_z, s);
+      else launch<4, 64, 80, 3, false>(maps, a, grid_z, s);
+      return;
     case kOzBuild:
       if (grid_z != 1) fail(DFJK_ERR_INVALID, "the two-SM build product takes one batch");
       launch_pair<5, 64, 96, 4>(maps, a, s);
       return;
-    case kOzSyrk: launch<5, 64, 96, 3>(maps, a, grid_z, s); return;
+    case kOzSyrk: launch<5, 64, 96, 3, false>(maps, a, grid_z, s); return;
   }
   fail(DFJK_ERR_INVALID, "unknown int8 GEMM shape %d", (int)shape);
 }
