@@ -51,15 +51,24 @@ __device__ __forceinline__ int row_exponent(double vmax) {
 // it (|t - d| <= 1/2).
 template <int ND>
 __device__ __forceinline__ void digits(double v, int e, int8_t* d) {
-  double t = ldexp(v, -e) * 128.0;
+  // v 2^(7-e): a power-of-two multiply while that power is a normal double
+  const int sh = 7 - e;
+  double t = (sh >= -1022 && sh <= 1023) ? v * __longlong_as_double((long long)(sh + 1023) << 52)
+                                         : ldexp(v, sh);
+  // round half to even by adding 1.5 * 2^52 (|t| < 2^31): the sum's low word
+  // is the integer and subtracting the constant back gives it as a double, so
+  // no float64 <-> int conversion is needed; t - q stays exact
+  constexpr double kRound = 6755399441055744.0;
   int q[ND];
-  q[0] = (int)rint(t);
-  t -= q[0];
+  double y = t + kRound;
+  q[0] = __double2loint(y);
+  t -= y - kRound;
 #pragma unroll
   for (int s = 1; s < ND; ++s) {
     t *= 256.0;
-    q[s] = (int)rint(t);
-    t -= q[s];
+    y = t + kRound;
+    q[s] = __double2loint(y);
+    t -= y - kRound;
   }
 #pragma unroll
   for (int s = ND - 1; s >= 1; --s)
