@@ -408,6 +408,24 @@ static void parse_basis(const dfjk_basis* b, const char* what, int lmax_supporte
 // Plan
 // ---------------------------------------------------------------------------
 
+// host threads for the plan tables (0 .. nth-1 each take [n t / nth, n (t+1) / nth))
+static int table_threads(int64_t n, int64_t min_chunk) {
+  const int64_t hw = std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(hw, n / min_chunk));
+}
+
+template <class F>
+static void for_ranges(int nth, int64_t n, F f) {
+  if (nth <= 1) {
+    f(0, (int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 1; t < nth; ++t) th.emplace_back(f, t, n * t / nth, n * (t + 1) / nth);
+  f(0, (int64_t)0, n / nth);
+  for (auto& x : th) x.join();
+}
+
 static void make_plan(Plan& p, const dfjk_basis* orb, const dfjk_basis* aux) {
   parse_basis(orb, "orbital", kLmaxOrb, false, p.orb, p.c2s_orb);
   parse_basis(aux, "auxiliary", kLmaxAux, true, p.aux, p.c2s_aux);
@@ -437,22 +455,29 @@ static void make_plan(Plan& p, const dfjk_basis* orb, const dfjk_basis* aux) {
   }
   // canonical orientation (larger l first) and class buckets
   struct PR { int l1, l2, s1, s2, a, b; };
-  std::vector<PR> prs;
-  prs.reserve(pa.size());
-  for (size_t i = 0; i < pa.size(); ++i) {
-    int a = pa[i], b = pb[i], s1 = a, s2 = b;
-    if (p.orb.l[a] < p.orb.l[b]) std::swap(s1, s2);
-    prs.push_back({p.orb.l[s1], p.orb.l[s2], s1, s2, a, b});
+  // stable order by (l1, l2): a counting sort over the 64 keys l1 * 8 + l2
+  std::vector<PR> prs(pa.size());
+  {
+    std::vector<int64_t> start(65, 0);
+    for (size_t i = 0; i < pa.size(); ++i) {
+      const int la = p.orb.l[pa[i]], lb = p.orb.l[pb[i]];
+      start[1 + std::max(la, lb) * 8 + std::min(la, lb)]++;
+    }
+    for (int k = 0; k < 64; ++k) start[k + 1] += start[k];
+    for (size_t i = 0; i < pa.size(); ++i) {
+      int a = pa[i], b = pb[i], s1 = a, s2 = b;
+      if (p.orb.l[a] < p.orb.l[b]) std::swap(s1, s2);
+      const int l1 = p.orb.l[s1], l2 = p.orb.l[s2];
+      prs[start[l1 * 8 + l2]++] = {l1, l2, s1, s2, a, b};
+    }
   }
-  std::stable_sort(prs.begin(), prs.end(), [](const PR& x, const PR& y) {
-    return x.l1 != y.l1 ? x.l1 < y.l1 : x.l2 < y.l2;
-  });
   p.classes.clear();
-  p.pair_s1.clear(); p.pair_s2.clear(); p.pair_orig_a.clear(); p.pair_orig_b.clear();
-  p.pair_row0.clear(); p.pair_pp0.clear(); p.pair_npp.clear();
-  std::vector<int> pp_pair, pp_pa, pp_pb;
+  const size_t npair = prs.size();
+  p.pair_s1.resize(npair); p.pair_s2.resize(npair); p.pair_orig_a.resize(npair);
+  p.pair_orig_b.resize(npair); p.pair_row0.resize(npair); p.pair_pp0.resize(npair);
+  p.pair_npp.resize(npair);
   int64_t row = 0, pp = 0, esph = 0;
-  for (size_t i = 0; i < prs.size(); ++i) {
+  for (size_t i = 0; i < npair; ++i) {
     const PR& r = prs[i];
     if (p.classes.empty() || p.classes.back().l1 != r.l1 || p.classes.back().l2 != r.l2) {
       ClassRange c{r.l1, r.l2, (int64_t)i, 0, pp, 0, esph};
@@ -460,20 +485,14 @@ static void make_plan(Plan& p, const dfjk_basis* orb, const dfjk_basis* aux) {
     }
     ClassRange& c = p.classes.back();
     c.count++;
-    p.pair_s1.push_back(r.s1);
-    p.pair_s2.push_back(r.s2);
-    p.pair_orig_a.push_back(r.a);
-    p.pair_orig_b.push_back(r.b);
-    p.pair_row0.push_back(row);
-    p.pair_pp0.push_back(pp);
+    p.pair_s1[i] = r.s1;
+    p.pair_s2[i] = r.s2;
+    p.pair_orig_a[i] = r.a;
+    p.pair_orig_b[i] = r.b;
+    p.pair_row0[i] = row;
+    p.pair_pp0[i] = pp;
     const int n1 = p.orb.nprim[r.s1], n2 = p.orb.nprim[r.s2];
-    p.pair_npp.push_back(n1 * n2);
-    for (int x = 0; x < n1; ++x)
-      for (int y = 0; y < n2; ++y) {
-        pp_pair.push_back((int)i);
-        pp_pa.push_back(x);
-        pp_pb.push_back(y);
-      }
+    p.pair_npp[i] = n1 * n2;
     pp += n1 * n2;
     c.pp_count += n1 * n2;
     const int na = 2 * r.l1 + 1, nb = 2 * r.l2 + 1;
@@ -484,34 +503,68 @@ static void make_plan(Plan& p, const dfjk_basis* orb, const dfjk_basis* aux) {
   p.nrows = row;
   p.npp = pp;
   p.esph_doubles = esph;
-  // rows -> (m, n), kinds, and K lists
+  // primitive pairs -> (pair, x, y) and rows -> (m, n), kinds: each range of
+  // pairs fills its own slices, in parallel
+  std::vector<int> pp_pair(pp), pp_pa(pp), pp_pb(pp);
   std::vector<int> rm(row), rn(row);
   std::vector<int8_t> kind(row);
-  std::vector<int> cnt(p.nao + 1, 0);
-  for (size_t i = 0; i < prs.size(); ++i) {
-    const int s1 = p.pair_s1[i], s2 = p.pair_s2[i];
-    const int na = 2 * p.orb.l[s1] + 1, nb = 2 * p.orb.l[s2] + 1;
-    for (int x = 0; x < na; ++x)
-      for (int y = 0; y < nb; ++y) {
-        const int64_t r = p.pair_row0[i] + x * nb + y;
-        const int m = p.orb.out0[s1] + x, n = p.orb.out0[s2] + y;
-        rm[r] = m;
-        rn[r] = n;
-        kind[r] = (s1 == s2) ? (m >= n ? 1 : 0) : 2;
-        cnt[m + 1]++;
-        if (kind[r] == 2) cnt[n + 1]++;
-      }
-  }
-  for (int m = 0; m < p.nao; ++m) cnt[m + 1] += cnt[m];
-  std::vector<int> krow(cnt[p.nao]), kn(cnt[p.nao]), fill(cnt.begin(), cnt.end() - 1);
-  for (int64_t r = 0; r < row; ++r) {
-    krow[fill[rm[r]]] = (int)r;
-    kn[fill[rm[r]]++] = rn[r];
-    if (kind[r] == 2) {
-      krow[fill[rn[r]]] = (int)r;
-      kn[fill[rn[r]]++] = rm[r];
+  for_ranges(table_threads((int64_t)npair, 4096), (int64_t)npair, [&](int, int64_t i0, int64_t i1) {
+    for (int64_t i = i0; i < i1; ++i) {
+      const int s1 = p.pair_s1[i], s2 = p.pair_s2[i];
+      const int n1 = p.orb.nprim[s1], n2 = p.orb.nprim[s2];
+      int64_t k = p.pair_pp0[i];
+      for (int x = 0; x < n1; ++x)
+        for (int y = 0; y < n2; ++y, ++k) {
+          pp_pair[k] = (int)i;
+          pp_pa[k] = x;
+          pp_pb[k] = y;
+        }
+      const int na = 2 * p.orb.l[s1] + 1, nb = 2 * p.orb.l[s2] + 1;
+      for (int x = 0; x < na; ++x)
+        for (int y = 0; y < nb; ++y) {
+          const int64_t r = p.pair_row0[i] + x * nb + y;
+          const int m = p.orb.out0[s1] + x, n = p.orb.out0[s2] + y;
+          rm[r] = m;
+          rn[r] = n;
+          kind[r] = (s1 == s2) ? (m >= n ? 1 : 0) : 2;
+        }
     }
+  });
+  // K lists: per m, the rows that touch m in ascending row order (a counting
+  // sort over row ranges; each range's histogram places its entries after
+  // those of the ranges before it, so the order is the sequential one)
+  const int nth = table_threads(row, 65536);
+  std::vector<std::vector<int>> hist(nth, std::vector<int>(p.nao, 0));
+  for_ranges(nth, row, [&](int t, int64_t r0, int64_t r1) {
+    std::vector<int>& h = hist[t];
+    for (int64_t r = r0; r < r1; ++r) {
+      h[rm[r]]++;
+      if (kind[r] == 2) h[rn[r]]++;
+    }
+  });
+  std::vector<int> cnt(p.nao + 1, 0);
+  for (int m = 0; m < p.nao; ++m) {
+    int acc = 0;
+    for (int t = 0; t < nth; ++t) {
+      const int h = hist[t][m];
+      hist[t][m] = acc;   // offset of range t within m's list
+      acc += h;
+    }
+    cnt[m + 1] = cnt[m] + acc;
   }
+  std::vector<int> krow(cnt[p.nao]), kn(cnt[p.nao]);
+  for_ranges(nth, row, [&](int t, int64_t r0, int64_t r1) {
+    std::vector<int> fill(p.nao);
+    for (int m = 0; m < p.nao; ++m) fill[m] = cnt[m] + hist[t][m];
+    for (int64_t r = r0; r < r1; ++r) {
+      krow[fill[rm[r]]] = (int)r;
+      kn[fill[rm[r]]++] = rn[r];
+      if (kind[r] == 2) {
+        krow[fill[rn[r]]] = (int)r;
+        kn[fill[rn[r]]++] = rm[r];
+      }
+    }
+  });
   // aux columns: shells sorted by l (stable), column runs per l
   p.aux_order.resize(p.aux.n);
   std::iota(p.aux_order.begin(), p.aux_order.end(), 0);
