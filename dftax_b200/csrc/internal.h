@@ -202,6 +202,7 @@ struct Plan {
   // build products
   int64_t nfit = 0, ldb = 0;
   int built = 0;
+  bool metric_ready = false;   // metric factor computed at creation, not yet used by a build
   DevBuf d_metric;   // naux x naux: V, then eigenvectors (column-major)
   DevBuf d_w;        // eigenvalues
   DevBuf d_L;        // naux x ldb factor (column-major, zero padded)

@@ -101,7 +101,11 @@ dfjk_status dfjk_trim(dfjk_ctx* ctx);
 /* Plan: shells, Schwarz-kept shell pairs, class buckets, device layout.
  * Replaces plan_eri3c / plan_pairs / _shell_pair_keep
  * (dftax/integrals/eri3c_bucketed.py:221-283, :448-483, :140-169) and the
- * cart2sph checks (:186-218). Synchronizes the context's device. */
+ * cart2sph checks (:186-218). It also computes the (P|Q) metric and its
+ * factor, on a stream of its own while the host builds the orbital tables,
+ * so that a metric failure (DFJK_ERR_NUMERIC) can come from here; the plan's
+ * first dfjk_build uses that factor and every later build recomputes it.
+ * Returns with its device work complete. */
 dfjk_status dfjk_plan_create(dfjk_ctx* ctx, const dfjk_basis* orb, const dfjk_basis* aux,
                              const dfjk_options* opts, dfjk_plan** plan);
 dfjk_status dfjk_plan_destroy(dfjk_plan* plan);
