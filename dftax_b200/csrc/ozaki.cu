@@ -45,39 +45,38 @@ __device__ __forceinline__ int row_exponent(double vmax) {
 // ND signed digits of t = v 2^-e (|t| < 1/2): a 7-bit leading digit, then
 // balanced 8-bit digits,
 //   t = d_0 2^-7 + sum_(s>=1) d_s 2^-(7+8s) + r,   |r| <= 2^-(8 ND),
-// with |d_0| <= 65 and -128 <= d_s <= 127 after the carries (a digit of +128
-// becomes -128 and carries one into the digit above). Every step is exact in
-// float64: scaling by a power of two, rounding to an integer and subtracting
-// it (|t - d| <= 1/2).
+// with |d_0| <= 65 and -128 <= d_s <= 127. They are the balanced base-256
+// digits of the integer N = rint(t 2^(7+8(ND-1))) (half to even, |N| < 2^39).
+// N comes from adding 1.5 * 2^52 to the exactly scaled value (the sum's
+// mantissa then holds N), with no float64 <-> int conversion; adding 128 to
+// every byte of N below the top digit turns each of those bytes into its
+// digit + 128, so the digits are read off with byte operations.
+template <int ND>
+__device__ __forceinline__ long long digit_biased(double v, int e) {
+  constexpr double kRound = 6755399441055744.0;   // 1.5 * 2^52
+  long long bias = 0;
+#pragma unroll
+  for (int s = 0; s < ND - 1; ++s) bias |= 128LL << (8 * s);
+  // v 2^sh: a power-of-two multiply while that power is a normal double
+  const int sh = 7 + 8 * (ND - 1) - e;
+  const double t = (sh >= -1022 && sh <= 1023)
+                       ? v * __longlong_as_double((long long)(sh + 1023) << 52)
+                       : ldexp(v, sh);
+  return __double_as_longlong(t + kRound) - __double_as_longlong(kRound) + bias;
+}
+
 template <int ND>
 __device__ __forceinline__ void digits(double v, int e, int8_t* d) {
-  // v 2^(7-e): a power-of-two multiply while that power is a normal double
-  const int sh = 7 - e;
-  double t = (sh >= -1022 && sh <= 1023) ? v * __longlong_as_double((long long)(sh + 1023) << 52)
-                                         : ldexp(v, sh);
-  // round half to even by adding 1.5 * 2^52 (|t| < 2^31): the sum's low word
-  // is the integer and subtracting the constant back gives it as a double, so
-  // no float64 <-> int conversion is needed; t - q stays exact
-  constexpr double kRound = 6755399441055744.0;
-  int q[ND];
-  double y = t + kRound;
-  q[0] = __double2loint(y);
-  t -= y - kRound;
+  const long long m = digit_biased<ND>(v, e);
 #pragma unroll
-  for (int s = 1; s < ND; ++s) {
-    t *= 256.0;
-    y = t + kRound;
-    q[s] = __double2loint(y);
-    t -= y - kRound;
-  }
-#pragma unroll
-  for (int s = ND - 1; s >= 1; --s)
-    if (q[s] > 127) {
-      q[s] -= 256;
-      q[s - 1] += 1;
-    }
-#pragma unroll
-  for (int s = 0; s < ND; ++s) d[s] = (int8_t)q[s];
+  for (int s = 1; s < ND; ++s) d[s] = (int8_t)(((m >> (8 * (ND - 1 - s))) & 0xFF) ^ 0x80);
+  d[0] = (int8_t)(m >> (8 * (ND - 1)));
+}
+
+// the four digits of digits<4> packed into a word, d_0 in the low byte
+__device__ __forceinline__ uint32_t digits4_word(double v, int e) {
+  const uint32_t m = (uint32_t)digit_biased<4>(v, e) ^ 0x808080u;   // bytes d_3 d_2 d_1 d_0
+  return __byte_perm(m, 0, 0x0123);
 }
 
 // Digit planes of the square B_x: A[d][x][m][nao_p] (4 digits) with row
@@ -140,12 +139,7 @@ __global__ void __launch_bounds__(256) kplanes_kernel(const double* __restrict__
   }
   __syncthreads();
   const int ex = sh_e[lx];
-  auto pack = [&](double v) {
-    int8_t d[4];
-    digits<4>(v, ex, d);
-    return (uint32_t)(uint8_t)d[0] | ((uint32_t)(uint8_t)d[1] << 8) | ((uint32_t)(uint8_t)d[2] << 16) |
-           ((uint32_t)(uint8_t)d[3] << 24);
-  };
+  auto pack = [&](double v) { return digits4_word(v, ex); };
   if (xin) {
     uint32_t* row = sw + lx * W;
     int e = e0 + g;
