@@ -279,6 +279,27 @@ def test_fp64_k_is_bitwise_reproducible():
     assert np.array_equal(K1, K1.T)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_first_build_uses_creation_metric_bitwise(precision):
+    """Plan creation computes the metric factor on a stream of its own and the
+    first build uses it; a second build recomputes it on the caller's stream.
+    Both builds give the same J and K, bit for bit, and the same kept count."""
+    from dftax_b200 import Plan, systems
+
+    sym, xyz, orb, aux, nocc = systems.workload("water8", seed=6)
+    plan = Plan(orb, aux, precision=precision)
+    C = systems.random_occupied(orb.nao, nocc, seed=9)
+    plan.build()
+    nfit1 = plan.info()["nfit"]
+    J1, K1 = (x.cpu().numpy() for x in plan.jk(C))
+    assert plan.phase_times()["metric"] > 0.0
+    plan.build()
+    J2, K2 = (x.cpu().numpy() for x in plan.jk(C))
+    assert plan.info()["nfit"] == nfit1
+    assert np.array_equal(J1, J2) and np.array_equal(K1, K2)
+    plan.close()
+
+
 def test_trim_and_rebuild(water_golden):
     """Cached device memory goes back to the driver; later plans still work."""
     from dftax_b200 import Context, Plan
