@@ -239,13 +239,21 @@ __global__ void __launch_bounds__(256) split_slices_kernel(const double* __restr
 }
 
 // K[i] = (beta0 ? 0 : K[i]) + sign * sum_z part[z][i], z in a fixed order
-__global__ void reduce_slices_kernel(const double* __restrict__ part, int64_t nslice, int64_t n,
+// K[m][j] = sign * sum_z part[z][m][j] (or += with beta0 = 0) for j <= m, in
+// slice order, mirrored to K[j][m]: the slice products computed only the
+// tiles that reach the lower triangle, and K comes out exactly symmetric
+__global__ void reduce_slices_kernel(const double* __restrict__ part, int64_t nslice, int64_t nao,
                                      double sign, int beta0, double* __restrict__ K) {
+  const int64_t n = nao * nao;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int64_t m = i / nao, j = i % nao;
+  if (j > m) return;
   double acc = 0.0;
   for (int64_t z = 0; z < nslice; ++z) acc += part[z * n + i];
+  const int64_t t = j * nao + m;
   K[i] = beta0 ? sign * acc : K[i] + sign * acc;
+  if (t != i) K[t] = beta0 ? sign * acc : K[t] + sign * acc;
 }
 
 // 4-digit planes of C'^T: Ct[d][i][n] from Cp[n][i] (nao x nsel), exponents eb[i]
@@ -469,6 +477,7 @@ void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, d
   a.ld_out = nao;
   a.batch_stride_out = nao * nao;
   a.err = p.ws_oz_err.as<int>();
+  a.lower = 1;
   for (int64_t z0 = 0; z0 < nsl; z0 += 65535) {
     const int64_t nz = std::min<int64_t>(65535, nsl - z0);
     a.plane0 = (int)z0;
@@ -476,8 +485,8 @@ void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, d
     ozaki_launch(kOzSyrk, maps, a, (int)nz, s);
   }
   const int64_t n = nao * nao;
-  reduce_slices_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p.ws_oz_kp.as<double>(), nsl, n,
-                                                                   sign, beta0 ? 1 : 0, K);
+  reduce_slices_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p.ws_oz_kp.as<double>(), nsl,
+                                                                   nao, sign, beta0 ? 1 : 0, K);
   DFJK_LAUNCHED();
   check_oz_err(p, s);
 }

@@ -45,6 +45,7 @@ struct OzakiArgs {
   int zper;                // batches per CTA (one TMEM allocation, one ring); 0 or 1: one
   int zcount;              // batches of the launch (set by ozaki_launch)
   int tma_out;             // half transform: 1 writes through maps.out (the build product always does)
+  int lower;               // 1: tiles wholly above the diagonal (n0 > m0 + 127) are skipped
 };
 
 // 3-D int8 tensor map over [d2][d1][d0] (d0 contiguous; strides in bytes),

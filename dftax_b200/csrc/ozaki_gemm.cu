@@ -223,6 +223,9 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
   const int zper = a.zper > 0 ? a.zper : 1;
   const int z0 = blockIdx.z * zper;
   const int nz = (a.zcount - z0) < zper ? (a.zcount - z0) : zper;   // batches of this CTA
+  // a symmetric product needs only the tiles that reach the lower triangle;
+  // the whole CTA leaves before any barrier or tensor memory is set up
+  if (a.lower && n0 > m0 + kBM - 1) return;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) {
