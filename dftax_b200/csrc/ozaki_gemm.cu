@@ -17,13 +17,15 @@
 //
 // Tiles: 128 (m) x BN (n) x BK (k, bytes), K-major operands, TMA with the
 // BK-byte swizzle into an ST-stage mbarrier ring (ND digit planes per operand
-// per stage). Two shapes are compiled: ND 4, BK 128, BN 80, two 104 KB stages
-// (K half transform: n = occupied orbitals, 160 = 2 x 80 for (H2O)_32), and
+// per stage). Two shapes are compiled: ND 4, BK 64, BN 80, three 52 KB stages
+// and 64 KB of output staging for TMA stores (K half transform: n = occupied
+// orbitals, 160 = 2 x 80 for (H2O)_32), and
 // ND 5, BK 64, BN 96, three 70 KB stages (K = X X^T; 5 x 96 of the 512 TMEM
 // columns). The build product runs on SM pairs (ozaki_gemm_i8_pair below,
 // M = 256, four 55 KB stages). Warp 0 lane 0 issues
-// copies, warp 1 lane 0 issues MMAs (BK/32 per digit pair per k tile), all
-// four warps drain tensor memory (warp w owns rows 32w..32w+31). Every wait
+// copies, warp 1 lane 0 issues MMAs (BK/32 per digit pair per k tile), and
+// eight warps drain tensor memory (warps w and w + 4 own rows 32 (w % 4) ..
+// + 31, alternate 16-column chunks each). Every wait
 // is bounded (4 s of %globaltimer); a timeout sets *err, skips the remaining
 // work, drains the copies in flight (bounded) and still frees the tensor
 // memory.
@@ -190,7 +192,7 @@ __device__ __forceinline__ void stage_row(uint8_t* buf, int lane, const uint32_t
 }
 
 template <int ND, int BK, int BN, int ST, bool TOUT>
-__global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ OzakiMaps maps,
+__global__ void __launch_bounds__(320, 1) ozaki_gemm_i8(const __grid_constant__ OzakiMaps maps,
                                                         OzakiArgs a) {
   constexpr uint32_t A_TILE = kBM * BK;
   constexpr uint32_t B_TILE = BN * BK;
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
   // TOUT: per epilogue warp two 32 x 16 float64 staging blocks after the ring
   // (outputs leave through maps.out); barriers: full[ST], empty[ST], done
   // (accumulators of a batch final), drained (the epilogue warps have read them)
-  constexpr uint32_t STG_BYTES = TOUT ? 4 * 2 * 4096 : 0;
+  constexpr uint32_t STG_BYTES = TOUT ? 8 * 2 * 4096 : 0;
   static_assert(BN % 16 == 0, "16-column epilogue chunks");
   uint8_t* stg = smem + ST * STAGE;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * STAGE + STG_BYTES);
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
       mbar_init(smem_u32(&empty[s]), 1);
     }
     mbar_init(smem_u32(done), 1);
-    mbar_init(smem_u32(drained), 4);
+    mbar_init(smem_u32(drained), 8);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -313,8 +315,9 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
       umma_commit(smem_u32(done));
     }
   } else if (warp >= 2) {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
-    const int q = warp & 3;
+    // epilogue, eight warps: warp w reads TMEM lanes 32 (w % 4) .. + 31 and
+    // the 16-column chunks h, h + 2, ... of them, h = (w - 2) / 4
+    const int q = warp & 3, h = (warp - 2) >> 2;
     const int row0 = m0 + q * 32, row = row0 + lane;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
     int nst = 0;   // TOUT: blocks this warp has handed to TMA (double buffer index)
@@ -338,7 +341,7 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
       const int era = row < a.M ? a.ea[(int64_t)(a.plane0 + z) * a.ea_stride + row] : 0;
       double* orow = a.out + (int64_t)z * a.batch_stride_out + (int64_t)row * a.ld_out;
       const int* ebz = a.eb + (int64_t)bz * a.eb_stride;
-      for (int c = 0; c < BN; c += 16) {
+      for (int c = 16 * h; c < BN; c += 32) {
         uint32_t v[ND][16];
 #pragma unroll
         for (int o = 0; o < ND; ++o) tmem_ld16_issue(trow + (uint32_t)o * ACC + c, v[o]);
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(192, 1) ozaki_gemm_i8(const __grid_constant__ 
           int ecol[16];
 #pragma unroll
           for (int j = 0; j < 16; ++j) ecol[j] = n0 + c + j < a.N ? ebz[n0 + c + j] : 0;
-          uint8_t* buf = stg + (uint32_t)(q * 2 + (nst & 1)) * 4096;
+          uint8_t* buf = stg + (uint32_t)((warp - 2) * 2 + (nst & 1)) * 4096;
           // the block handed over two chunks ago has been read out of this buffer
           if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
           __syncwarp();
@@ -640,7 +643,7 @@ EncodeTiled encode_fn() {
 
 template <int ND, int BK, int BN, int ST, bool TOUT>
 constexpr size_t smem_bytes() {
-  return (size_t)ST * ND * (kBM * BK + BN * BK) + (TOUT ? 4 * 2 * 4096 : 0) + 1024 + 256;
+  return (size_t)ST * ND * (kBM * BK + BN * BK) + (TOUT ? 8 * 2 * 4096 : 0) + 1024 + 256;
 }
 
 template <int ND, int BK, int BN, int ST, bool TOUT>
@@ -653,7 +656,7 @@ void launch(const OzakiMaps& maps, const OzakiArgs& a, int grid_z, cudaStream_t 
   dim3 grid((a.N + BN - 1) / BN, (a.M + kBM - 1) / kBM, (grid_z + b.zper - 1) / b.zper);
   DFJK_CUDA(cudaFuncSetAttribute(ozaki_gemm_i8<ND, BK, BN, ST, TOUT>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ozaki_gemm_i8<ND, BK, BN, ST, TOUT><<<grid, 192, smem, s>>>(maps, b);
+  ozaki_gemm_i8<ND, BK, BN, ST, TOUT><<<grid, 320, smem, s>>>(maps, b);
   DFJK_LAUNCHED();
 }
 
