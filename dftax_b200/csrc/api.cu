@@ -809,7 +809,10 @@ void build(Plan& p, cudaStream_t s) {
     }
     p.timer.mark(kPhBgemm, s);
   }
-  check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
+  // float64: a non-finite integral or factor propagates into B; mixed: the
+  // digit splits flagged any non-finite input (a NaN's digits are finite)
+  if (mixed) ozaki_check(p, s);
+  else check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
   if (mixed) {
     p.timer.mark(kPhKplanes, s);
     build_ozaki_planes(p, s);

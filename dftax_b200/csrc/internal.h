@@ -226,6 +226,9 @@ struct Plan {
 
 // ---- mixed precision on the int8 tensor cores (ozaki.cu) ----
 void ozaki_prepare_l(Plan& p, cudaStream_t s);
+// error flag of the tensor-core pipeline and non-finite inputs of the digit
+// splits since ozaki_prepare_l (one host synchronization)
+void ozaki_check(Plan& p, cudaStream_t s);
 void ozaki_split_raw(Plan& p, const double* raw, int64_t nr, int8_t* planes, int64_t plane_stride,
                      int* e, cudaStream_t s);
 void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int* e, int64_t nr,

@@ -183,14 +183,21 @@ __global__ void __launch_bounds__(256) split_rows_kernel(const double* __restric
                                                          int64_t ncols, int64_t kp,
                                                          int* __restrict__ e_out,
                                                          int64_t plane_stride,
-                                                         int8_t* __restrict__ planes) {
+                                                         int8_t* __restrict__ planes,
+                                                         int* __restrict__ nonfinite) {
   __shared__ double red[256];
   const int64_t row = blockIdx.x;
   const double* r = src + row * ld;
   double mx = 0.0;
-  for (int64_t k = threadIdx.x; k < ncols; k += 256) mx = fmax(mx, fabs(r[k]));
+  bool bad = false;
+  for (int64_t k = threadIdx.x; k < ncols; k += 256) {
+    const double v = r[k];
+    bad |= !isfinite(v);
+    mx = fmax(mx, fabs(v));
+  }
   red[threadIdx.x] = mx;
-  __syncthreads();
+  // digits of a NaN or infinity would be finite and wrong: the caller is told
+  if (__syncthreads_or(bad) && threadIdx.x == 0 && nonfinite) atomicExch(nonfinite, 1);
   for (int o = 128; o > 0; o >>= 1) {
     if ((int)threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
     __syncthreads();
@@ -327,12 +334,25 @@ void ozaki_prepare_l(Plan& p, cudaStream_t s) {
   p.ws_oz_l.ensure((size_t)kOzBDigits * plane);
   p.ws_oz_el.ensure((size_t)p.ldb * sizeof(int));
   // L is column-major naux x ldb: column x (contiguous over P) is row x of L^T
+  // one flag for every digit split of this build (L and the raw rows),
+  // read with the pipeline's error flag by ozaki_check at the end
+  p.ws_flag.ensure(sizeof(int));
+  DFJK_CUDA(cudaMemsetAsync(p.ws_flag.p, 0, sizeof(int), s));
   split_rows_kernel<kOzBDigits><<<(unsigned)p.ldb, 256, 0, s>>>(
       p.d_L.as<double>(), p.naux, p.naux, p.naux_p16, p.ws_oz_el.as<int>(), plane,
-      p.ws_oz_l.as<int8_t>());
+      p.ws_oz_l.as<int8_t>(), p.ws_flag.as<int>());
   DFJK_LAUNCHED();
   p.ws_oz_err.ensure(sizeof(int));
   DFJK_CUDA(cudaMemsetAsync(p.ws_oz_err.p, 0, sizeof(int), s));
+}
+
+void ozaki_check(Plan& p, cudaStream_t s) {
+  int h[2] = {0, 0};
+  DFJK_CUDA(cudaMemcpyAsync(&h[0], p.ws_oz_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaMemcpyAsync(&h[1], p.ws_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  if (h[0]) fail(DFJK_ERR_CUDA, "tensor-core pipeline gave up waiting (code %d)", h[0]);
+  if (h[1]) fail(DFJK_ERR_NUMERIC, "non-finite values in the 3-center integrals or the metric factor");
 }
 
 // Digit planes of nr raw 3-center rows (ld naux): planes[d * plane_stride +
@@ -342,7 +362,8 @@ void ozaki_split_raw(Plan& p, const double* raw, int64_t nr, int8_t* planes, int
   if (nr <= 0) return;
   p.naux_p16 = (p.naux + 15) / 16 * 16;
   split_rows_kernel<kOzBDigits><<<(unsigned)nr, 256, 0, s>>>(raw, p.naux, p.naux, p.naux_p16, e,
-                                                             plane_stride, planes);
+                                                             plane_stride, planes,
+                                                             p.ws_flag.as<int>());
   DFJK_LAUNCHED();
 }
 
@@ -382,7 +403,7 @@ void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int*
     a.out = Bout + m0 * p.ldb;
     ozaki_launch(kOzBuild, maps, a, 1, s);
   }
-  check_oz_err(p, s);
+  // checked once per build (ozaki_check)
 }
 
 void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s) {
