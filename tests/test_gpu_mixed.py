@@ -153,3 +153,29 @@ def test_mixed_open_shell_vs_fp64():
     assert abs(emx - e64) < E_ABS
     for s in range(2):
         assert rel(Fmx[s].cpu().numpy(), F64[s].cpu().numpy()) < K_REL
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_build_reports_overflowing_integrals(water_golden, precision):
+    """A contraction coefficient of 1e300 is finite, but the (aa|P) integrals
+    it enters overflow. The int8 digits of an infinity would be finite, so the
+    mixed build flags non-finite raw rows while splitting them; the float64
+    build finds them in B. Either way the build reports NUMERIC and the
+    context stays usable."""
+    from dftax_b200 import Plan
+    from dftax_b200._lib import DfjkError
+
+    g = water_golden
+    orb, aux = golden_basis(g, "orb"), golden_basis(g, "aux")
+    big = golden_basis(g, "orb")
+    big.coefficients = big.coefficients.copy()
+    big.coefficients[0, 0] = 1e300
+    p = Plan(big, aux, precision=precision)
+    with pytest.raises(DfjkError) as ei:
+        p.build()
+    assert ei.value.status_name == "NUMERIC"
+    p.close()
+    ok = Plan(orb, aux, precision=precision).build()
+    J, _ = ok.jk(g["C"])
+    assert np.isfinite(J.cpu().numpy()).all()
+    ok.close()
