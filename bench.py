@@ -359,6 +359,12 @@ def run_ours(args, rank, world, local_rank):
     h2d = sum(a.nbytes for b in (orb, aux) for a in (b.centers, b.exponents, b.coefficients,
                                                       b.angular, b.cart2sph)) + C.nbytes
     d2h = Jh.nbytes + Kh.nbytes
+    # one untimed step first, like the warm-up of the device-resident step (the
+    # other precision's plans left differently sized buffers in the cache)
+    p2 = Plan(orb, aux, precision=head)
+    p2.build(stream)
+    p2.jk_host(C, J=Jh, K=Kh, stream=stream)
+    p2.close()
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
