@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--screen", type=float, default=0.0,
+                    help="relative Schwarz screen of shell pairs (0: none, the default)")
     return ap.parse_args()
 
 
@@ -321,7 +323,7 @@ def run_ours(args, rank, world, local_rank):
     lib = _lib.load()
     res = {}
     for prec in precs:
-        plan = Plan(orb, aux, precision=prec)
+        plan = Plan(orb, aux, precision=prec, screen=args.screen or None)
         J = torch.empty((orb.nao, orb.nao), dtype=torch.float64, device="cuda")
         K = torch.empty_like(J)
 
@@ -361,7 +363,7 @@ def run_ours(args, rank, world, local_rank):
     d2h = Jh.nbytes + Kh.nbytes
     # one untimed step first, like the warm-up of the device-resident step (the
     # other precision's plans left differently sized buffers in the cache)
-    p2 = Plan(orb, aux, precision=head)
+    p2 = Plan(orb, aux, precision=head, screen=args.screen or None)
     p2.build(stream)
     p2.jk_host(C, J=Jh, K=Kh, stream=stream)
     p2.close()
@@ -370,7 +372,7 @@ def run_ours(args, rank, world, local_rank):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.e2e_steps):
-        p2 = Plan(orb, aux, precision=head)
+        p2 = Plan(orb, aux, precision=head, screen=args.screen or None)
         p2.build(stream)
         p2.jk_host(C, J=Jh, K=Kh, stream=stream)
         p2.close()
@@ -435,7 +437,7 @@ def run_ours(args, rank, world, local_rank):
         "dtype": "f64+i8" if mixed else "f64", "data": "synthetic",
         "config": {"workload": f"{args.workload} one DF J/K build from geometry (seeded)",
                    "nao": nao, "naux": naux, "nocc": nocc, "nfit": nfit, "nrows": nrows,
-                   "precision": head, "parallelism": f"replicas x{world}",
+                   "precision": head, "screen": args.screen, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (B is %.1f GB)" % (8.0 * nrows * ldb / 1e9)},
         "phases_ms": {k: round(v, 3) for k, v in phases.items()},
         "jk_iteration": {"value": round(1e3 / r["jk_ms"], 3), "unit": "J/K builds/s with B resident",
