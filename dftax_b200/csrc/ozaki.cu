@@ -419,7 +419,12 @@ void ozaki_prepare_c(Plan& p, const double* Cp, int64_t nsel, cudaStream_t s) {
 // X[m][x - x0][i] (float64, ld n * nsel) for fitted directions [x0, x0 + n)
 void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStream_t s) {
   constexpr int ND = kOzKDigits;
-  const OzakiShapeInfo sh = ozaki_shape(kOzHalf);
+  // every tile of occupied columns streams all B_x planes: take 96-column
+  // tiles when they need fewer tiles than 80-column ones (81 columns: 1, not 2)
+  const int64_t t80 = (nsel + ozaki_shape(kOzHalf).bn - 1) / ozaki_shape(kOzHalf).bn;
+  const int64_t t96 = (nsel + ozaki_shape(kOzHalfWide).bn - 1) / ozaki_shape(kOzHalfWide).bn;
+  const OzakiShape shape = t96 < t80 ? kOzHalfWide : kOzHalf;
+  const OzakiShapeInfo sh = ozaki_shape(shape);
   const int bk = sh.box_k;
   const int64_t nao = p.nao, nao_p = p.nao_p16;
   const int64_t plane = p.nfit * nao * nao_p;
@@ -455,7 +460,7 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
     // X[m][z][i] leaves through TMA tensor stores when its strides allow
     a.tma_out = ozaki_out_mappable(a.out, a.batch_stride_out, a.ld_out) ? 1 : 0;
     if (a.tma_out) ozaki_map_out(&maps.out, a.out, nsel, nz, nao, a.batch_stride_out, a.ld_out);
-    ozaki_launch(kOzHalf, maps, a, (int)nz, s);
+    ozaki_launch(shape, maps, a, (int)nz, s);
   }
   check_oz_err(p, s);
 }

@@ -17,7 +17,9 @@ constexpr int64_t kOzMaxK = 32640;
 constexpr int64_t kOzSlice = 8192;  // k bytes per slice of the K = X X^T product
 
 // The products and the tile shape each one runs with (ozaki_gemm.cu).
-enum OzakiShape { kOzBuild = 0, kOzHalf = 1, kOzSyrk = 2 };
+// kOzHalfWide: the half transform with 96 occupied columns per tile, used when
+// it needs fewer tiles than 80 columns would (each tile streams every B_x plane)
+enum OzakiShape { kOzBuild = 0, kOzHalf = 1, kOzSyrk = 2, kOzHalfWide = 3 };
 struct OzakiShapeInfo {
   int digits, box_k, bn, stages;   // digits per value, k tile bytes, n tile, ring depth
   int box_b;                       // B rows per copy: bn, or bn / 2 on SM pairs

@@ -701,6 +701,7 @@ void launch_pair(const OzakiMaps& maps, const OzakiArgs& a, cudaStream_t s) {
 OzakiShapeInfo ozaki_shape(OzakiShape shape) {
   switch (shape) {
     case kOzHalf: return {kOzKDigits, 64, 80, 3, 80};
+    case kOzHalfWide: return {kOzKDigits, 64, 96, 2, 96};
     case kOzBuild: return {kOzBDigits, 64, 96, 4, 48};
     case kOzSyrk: return {kOzSDigits, 64, 96, 3, 96};
   }
@@ -751,6 +752,11 @@ void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, i
     case kOzHalf:
       if (a.tma_out) launch<4, 64, 80, 3, true>(maps, a, grid_z, s);
       else launch<4, 64, 80, 3, false>(maps, a, grid_z, s);
+      return;
+    case kOzHalfWide:
+      // two stages: three would not leave room for the output staging
+      if (a.tma_out) launch<4, 64, 96, 2, true>(maps, a, grid_z, s);
+      else launch<4, 64, 96, 2, false>(maps, a, grid_z, s);
       return;
     case kOzBuild:
       if (grid_z != 1) fail(DFJK_ERR_INVALID, "the two-SM build product takes one batch");

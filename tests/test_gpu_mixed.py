@@ -55,9 +55,12 @@ def test_mixed_jk_and_energy_vs_reference(name):
     assert rel(F[0].cpu().numpy(), 2.0 * g["J"] - 0.25 * g["K"]) < K_REL
 
 
-@pytest.mark.parametrize("name,ncol", [("water8", None), ("water8", 100), ("alkane2", None)])
+@pytest.mark.parametrize("name,ncol", [("water8", None), ("water8", 100), ("water8", 90),
+                                      ("water8", 91), ("alkane2", None)])
 def test_mixed_vs_fp64(name, ncol):
-    """Several 128-row and 80-column tiles (nao 240; 100 columns), f shells."""
+    """Several 128-row and 80-column tiles (nao 240; 100 columns), f shells;
+    90 and 91 columns take one 96-column tile in the half transform (91
+    columns, a row pitch TMA cannot store, with direct stores)."""
     from dftax_b200 import systems
 
     sym, xyz, orb, aux, nocc = systems.workload(name, seed=3)
