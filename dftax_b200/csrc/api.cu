@@ -203,7 +203,8 @@ void standard_block(int l, std::vector<double>& out) {
           const double sign = ((t + (tv - vm2) / 2) % 2) ? -1.0 : 1.0;
           const double c = sign * std::pow(0.25, t) * binom(l, t) * binom(l - t, am + t) *
                            binom(t, u) * binom(am, tv);
-          const int py = 2 * u + tv, px = 2 * t + am - 2 * u - tv, pz = l - 2 * t - am;
+          // the z power is l - px - py = l - 2t - am
+          const int py = 2 * u + tv, px = 2 * t + am - 2 * u - tv;
           out[comp_index(l, px, py) * ns + col] += c * nrm;
         }
       }

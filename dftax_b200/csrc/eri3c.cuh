@@ -228,7 +228,7 @@ __device__ __forceinline__ double boys_order(int n, double t, const double* __re
 template <int LA, int LB, int LC>
 __global__ void __launch_bounds__(128) eri3c_coop_kernel(Eri3cArgs a) {
   using S = CoopShape<LA, LB, LC>;
-  constexpr int NC = S::NC, NCC = S::NCC, LAB = S::LAB, M = S::M, NH = S::NH, NR = S::NR;
+  constexpr int NC = S::NC, NCC = S::NCC, M = S::M, NH = S::NH, NR = S::NR;
   constexpr int NAB = S::NAB, NHP = S::NHP;
   constexpr int RJ = (NR + 31) / 32, HJ = (NH + 31) / 32;
   static_assert(NAB <= 64, "two bra rows per lane");
