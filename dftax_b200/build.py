@@ -11,6 +11,7 @@ from __future__ import annotations
 import concurrent.futures as cf
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -31,14 +32,28 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _deps():
-    return sorted(glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))
-                  + glob.glob(os.path.join(os.path.dirname(HERE), "include", "*.h")))
+_INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src: str) -> list[str]:
+    """Local headers that src includes, directly or through other headers."""
+    seen: set[str] = set()
+    todo = [src]
+    while todo:
+        f = todo.pop()
+        with open(f) as fh:
+            text = fh.read()
+        for name in _INC.findall(text):
+            h = os.path.normpath(os.path.join(os.path.dirname(f), name))
+            if os.path.exists(h) and h not in seen:
+                seen.add(h)
+                todo.append(h)
+    return sorted(seen)
 
 
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(OUT, os.path.basename(src) + ".o")
-    newest = max([os.path.getmtime(src)] + [os.path.getmtime(d) for d in _deps()])
+    newest = max([os.path.getmtime(src)] + [os.path.getmtime(d) for d in _deps(src)])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return obj
     cmd = [nvcc(), *ARCH, *FLAGS, "-c", src, "-o", obj]

@@ -912,24 +912,6 @@ double energy(Plan& p, const double* P, int nspin, double hf, double hf_lr, doub
 
 using namespace dfjk;
 
-template <class Fn>
-static dfjk_status guard(Context* c, Fn&& fn) {
-  try {
-    fn();
-    if (c) c->last_error.clear();
-    return DFJK_OK;
-  } catch (const Error& e) {
-    if (c) c->last_error = e.msg;
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    if (c) c->last_error = "host allocation failed";
-    return DFJK_ERR_MEMORY;
-  } catch (const std::exception& e) {
-    if (c) c->last_error = e.what();
-    return DFJK_ERR_INVALID;
-  }
-}
-
 static cudaStream_t st(void* s) { return static_cast<cudaStream_t>(s); }
 
 extern "C" {
@@ -956,6 +938,9 @@ dfjk_status dfjk_create(int device, dfjk_ctx** out) {
     h->c.device = device;
     DFJK_CUBLAS(cublasCreate(&h->c.cublas));
     DFJK_CUSOLVER(cusolverDnCreate(&h->c.cusolver));
+    // the no-alloc J path's fixed scratch: its module is loaded (and the array
+    // placed in device memory) here, not in that path's first call
+    h->c.noalloc_scratch = noalloc_scratch_address();
     std::vector<double> tbl, asym;
     boys_table_host(tbl, asym);
     upload(h->c.boys, tbl);

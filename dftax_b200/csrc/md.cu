@@ -14,6 +14,7 @@
 //     contiguous column runs of one row.
 #include "eri3c.cuh"
 #include "md_device.cuh"
+#include "internal.h"
 
 #include <cmath>
 

@@ -4,7 +4,7 @@
 // (:290-369) and dftax/energy/boys.py (:130-176).
 #pragma once
 
-#include "internal.h"
+#include "common.h"
 
 #include <type_traits>
 #include <utility>

@@ -13,19 +13,17 @@
 //   * the scratch holds kParts partial rows of gamma plus gamma itself, for B
 //     with at most kMaxFit columns (the plan's fitted dimension rounded up to
 //     8); larger plans are rejected with DFJK_ERR_UNSUPPORTED. Its size is
-//     (kParts + 1) * kMaxFit doubles = 16.8 MB, held by every GPU that loads
-//     the library until the process exits;
+//     (kParts + 1) * kMaxFit doubles = 16.8 MB per device. dfjk_create looks
+//     up its address with the context's device current, which loads this
+//     file's module: the 16.8 MB are taken then, not by a later call of the
+//     entry point, and stay until the process exits;
 //   * every call on a device uses the same array and leaves its contents
 //     behind; each call overwrites all the scratch it reads, so nothing needs
 //     clearing, but two calls whose kernels overlap on the GPU (different
-//     streams, no ordering between them) race on it;
-//   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current); make that first call
-//     before any stream capture.
+//     streams, no ordering between them) race on it.
 #include "internal.h"
 
 #include <algorithm>
-#include <mutex>
 
 namespace dfjk {
 namespace {
@@ -37,24 +35,6 @@ constexpr int kCols = kThreads * 8;          // columns per CTA (4 double2 per t
 constexpr int kRowBatch = 32;                // rows whose density weights a CTA stages at once
 
 __device__ __align__(256) double g_scratch[(kParts + 1) * kMaxFit];
-
-double* g_scratch_addr[64] = {nullptr};
-std::mutex g_scratch_mu;
-
-// Device address of g_scratch for the current device (looked up once).
-double* scratch_for_device(int dev) {
-  if (dev < 0 || dev >= 64) fail(DFJK_ERR_INVALID, "device %d out of range for the no-alloc path", dev);
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
-    if (e != cudaSuccess)
-      fail(DFJK_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
-           cudaGetErrorString(e));
-    g_scratch_addr[dev] = static_cast<double*>(ptr);
-  }
-  return g_scratch_addr[dev];
-}
 
 // Partial gamma over a row range; the density weight of each row,
 // w_r sum_i w_i C[m][i] C[n][i], is formed in the CTA (no dvec array).
@@ -143,14 +123,23 @@ __global__ void j_rows_noalloc(const double* __restrict__ B, int64_t ldb, int64_
 
 }  // namespace
 
+double* noalloc_scratch_address() {
+  void* ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
+  if (e != cudaSuccess)
+    fail(DFJK_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
+         cudaGetErrorString(e));
+  return static_cast<double*>(ptr);
+}
+
 void j_noalloc(Plan& p, const double* C, const double* w, int64_t ncol, double* J, cudaStream_t s) {
   if (p.ldb > kMaxFit)
     fail(DFJK_ERR_UNSUPPORTED,
          "dfjk_j_noalloc supports at most %lld fitted columns; this plan has %lld (use dfjk_jk)",
          (long long)kMaxFit, (long long)p.ldb);
-  int dev = 0;
-  DFJK_CUDA(cudaGetDevice(&dev));
-  double* scratch = scratch_for_device(dev);
+  double* scratch = p.ctx->noalloc_scratch;
+  if (!scratch) fail(DFJK_ERR_STATE, "the context has no no-alloc scratch address");
+  const int dev = p.ctx->device;
   double* part = scratch;
   double* gamma = scratch + (int64_t)kParts * kMaxFit;
   DFJK_CUDA(cudaMemsetAsync(J, 0, (size_t)p.nao * p.nao * sizeof(double), s));
@@ -180,17 +169,12 @@ extern "C" dfjk_status dfjk_j_noalloc(dfjk_plan* pl, const double* C, const doub
                                       double* J, void* stream) {
   if (!pl) return DFJK_ERR_INVALID;
   dfjk::Context* c = pl->p.ctx;
-  try {
+  return dfjk::guard(c, [&] {
     if (!pl->p.built) dfjk::fail(DFJK_ERR_STATE, "dfjk_j_noalloc before dfjk_build");
     if (!C || !J || ncol <= 0) dfjk::fail(DFJK_ERR_INVALID, "C or J is null or ncol=%lld", (long long)ncol);
     if (pl->p.opts.precision != DFJK_FP64)
       dfjk::fail(DFJK_ERR_UNSUPPORTED, "dfjk_j_noalloc needs a float64 plan");
     DFJK_CUDA(cudaSetDevice(c->device));
     dfjk::j_noalloc(pl->p, C, w, ncol, J, static_cast<cudaStream_t>(stream));
-    c->last_error.clear();
-    return DFJK_OK;
-  } catch (const dfjk::Error& e) {
-    c->last_error = e.msg;
-    return e.code;
-  }
+  });
 }

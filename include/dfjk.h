@@ -160,8 +160,9 @@ dfjk_status dfjk_energy_rsh(dfjk_plan* plan, const double* P, int32_t nspin, dou
  * Scratch is a fixed 16.8 MB array in the library's device memory, shared by
  * all calls: plans whose B has more than 8192 columns are rejected
  * (DFJK_ERR_UNSUPPORTED), and calls that overlap on the GPU race on it. The
- * first call on a device looks up that array's address; make it before any
- * stream capture. Float64 plans only. */
+ * array is placed on a device when dfjk_create makes a context there (its
+ * address is looked up then) and is held until the process exits, so this
+ * call itself takes no device memory. Float64 plans only. */
 dfjk_status dfjk_j_noalloc(dfjk_plan* plan, const double* C, const double* w, int64_t ncol,
                            double* J, void* stream);
 

@@ -22,6 +22,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _noalloc_j(plan, C):
+    """J from dfjk_j_noalloc, and the device's free bytes before and after the
+    call (inputs and output are allocated before the first reading)."""
     import torch
 
     from dftax_b200 import _lib
@@ -29,10 +31,13 @@ def _noalloc_j(plan, C):
     Cd = torch.as_tensor(np.ascontiguousarray(C), device=plan.dev)
     J = torch.full((C.shape[0], C.shape[0]), np.nan, dtype=torch.float64, device=plan.dev)
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
     st = plan.lib.dfjk_j_noalloc(plan.h, Cd.data_ptr(), None, C.shape[1], J.data_ptr(), stream)
     _lib.check(st, plan.ctx.h)
     torch.cuda.synchronize()
-    return J.cpu().numpy()
+    free1, _ = torch.cuda.mem_get_info()
+    return J.cpu().numpy(), free0 - free1
 
 
 @pytest.mark.parametrize("workload", ["golden-water", "water8"])
@@ -47,7 +52,10 @@ def test_noalloc_j_matches_jk_twice(workload, water_golden):
     plan = Plan(orb, aux).build()
     for seed in (11, 12):   # two calls in a row: the shared scratch keeps the first call's data
         C = systems.random_occupied(orb.nao, nocc, seed=seed)
-        J = _noalloc_j(plan, C)
+        J, taken = _noalloc_j(plan, C)
+        # the call itself takes no device memory (the scratch was placed on the
+        # device when the context was created)
+        assert taken == 0
         Jref, _ = plan.jk(C, want_k=False)
         Jref = Jref.cpu().numpy()
         assert np.all(np.isfinite(J))
