@@ -2,7 +2,7 @@
 
 Run from the repository root, in a checkout that has the reference sources:
 
-    python tests/golden/make_golden.py [--ref PATH_TO_DFTAX_CHECKOUT]
+    python tests/golden/make_golden.py --ref PATH_TO_DFTAX_CHECKOUT
 
 dftax needs JAX, which is not installed here; ``jax_numpy_shim`` stands in for
 the handful of JAX features the DF path uses, so every number in the fixtures
@@ -233,7 +233,7 @@ def make_rsh(R, out, omega=0.3, hf=0.2, hf_lr=0.8, seed=0, nocc=5):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="path of a dftax checkout")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     R = load_reference(a.ref)
