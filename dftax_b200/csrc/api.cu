@@ -753,7 +753,6 @@ static int64_t rows_of(const Plan& p, int64_t b, int64_t e) {
 }
 
 void build(Plan& p, cudaStream_t s) {
-  Context& c = *p.ctx;
   p.built = 0;
   // the first build of a plan uses the metric factor computed while the plan
   // was created (same code and inputs); every later build recomputes it
@@ -783,13 +782,12 @@ void build(Plan& p, cudaStream_t s) {
   for (auto& ch : chunks) maxrows = std::max(maxrows, rows_of(p, ch.first, ch.second));
   DevBuf& raw = p.ws_raw;
   raw.ensure((size_t)maxrows * ld * sizeof(double));
-  if (mixed) {
-    ozaki_prepare_l(p, s);
-    p.ws_oz_raw.ensure((size_t)kOzBDigits * maxrows * kp);
-    p.ws_oz_er.ensure((size_t)maxrows * sizeof(int));
-  }
-  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
-  const double one = 1.0, zero = 0.0;
+  // B = (ij|P) L on the int8 tensor cores with exact accumulation: 5 digits
+  // per value in mixed precision, 7 (2^-56 of each row's scale, below
+  // float64's own rounding of the row maximum) for float64 plans
+  ozaki_prepare_l(p, s);
+  p.ws_oz_raw.ensure((size_t)build_digits(p) * maxrows * kp);
+  p.ws_oz_er.ensure((size_t)maxrows * sizeof(int));
   for (auto& ch : chunks) {
     const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
     p.timer.mark(kPhEri3c, s);
@@ -797,23 +795,16 @@ void build(Plan& p, cudaStream_t s) {
     p.timer.mark(kPhEri3c, s);
     // B[r0:r0+nr, :] = raw (nr x naux) . L (naux x ldb)
     p.timer.mark(kPhBgemm, s);
-    if (mixed) {
-      ozaki_split_raw(p, raw.as<double>(), nr, p.ws_oz_raw.as<int8_t>(), nr * kp,
-                      p.ws_oz_er.as<int>(), s);
-      ozaki_bgemm(p, p.ws_oz_raw.as<int8_t>(), nr * kp, p.ws_oz_er.as<int>(), nr,
-                  p.d_B.as<double>() + r0 * p.ldb, s);
-    } else {
-      // column-major view: B^T = L^T raw^T
-      DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)p.ldb, (int)nr, (int)p.naux,
-                              &one, p.d_L.as<double>(), (int)p.naux, raw.as<double>(), (int)ld,
-                              &zero, p.d_B.as<double>() + r0 * p.ldb, (int)p.ldb));
-    }
+    ozaki_split_raw(p, raw.as<double>(), nr, p.ws_oz_raw.as<int8_t>(), nr * kp,
+                    p.ws_oz_er.as<int>(), s);
+    ozaki_bgemm(p, p.ws_oz_raw.as<int8_t>(), nr * kp, p.ws_oz_er.as<int>(), nr,
+                p.d_B.as<double>() + r0 * p.ldb, s);
     p.timer.mark(kPhBgemm, s);
   }
-  // float64: a non-finite integral or factor propagates into B; mixed: the
-  // digit splits flagged any non-finite input (a NaN's digits are finite)
-  if (mixed) ozaki_check(p, s);
-  else check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
+  // the digit splits flagged any non-finite input (a NaN's digits are
+  // finite); float64 plans also scan B for an overflow in the product
+  ozaki_check(p, s);
+  if (!mixed) check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
   if (mixed) {
     p.timer.mark(kPhKplanes, s);
     build_ozaki_planes(p, s);
@@ -998,10 +989,14 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
       make_plan(lr->p, orb, aux);
     }
     // the int8 products are exact for dot products of at most kOzMaxK terms
+    // (kOzMaxK7 for the 7-digit build product of float64 plans)
     if (pl->p.opts.precision == DFJK_MIXED &&
         (pl->p.naux > kOzMaxK || pl->p.nao > kOzMaxK))
       fail(DFJK_ERR_UNSUPPORTED, "mixed precision supports nao, naux <= %lld (got %d, %d)",
            (long long)kOzMaxK, pl->p.nao, pl->p.naux);
+    if (pl->p.opts.precision == DFJK_FP64 && pl->p.naux > kOzMaxK7)
+      fail(DFJK_ERR_UNSUPPORTED, "float64 plans support naux <= %lld (got %d)",
+           (long long)kOzMaxK7, pl->p.naux);
   });
   if (r != DFJK_OK) {
     delete pl->p.lr;

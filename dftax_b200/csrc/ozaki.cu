@@ -51,6 +51,9 @@ __device__ __forceinline__ int row_exponent(double vmax) {
 // mantissa then holds N), with no float64 <-> int conversion; adding 128 to
 // every byte of N below the top digit turns each of those bytes into its
 // digit + 128, so the digits are read off with byte operations.
+// With 7 digits N reaches 2^54, past the 2^51 where adding 1.5 * 2^52
+// rounds correctly: there the exactly scaled value is converted to an integer
+// with round-half-even (cvt.rni.s64.f64), which is exact below 2^63.
 template <int ND>
 __device__ __forceinline__ long long digit_biased(double v, int e) {
   constexpr double kRound = 6755399441055744.0;   // 1.5 * 2^52
@@ -62,6 +65,7 @@ __device__ __forceinline__ long long digit_biased(double v, int e) {
   const double t = (sh >= -1022 && sh <= 1023)
                        ? v * __longlong_as_double((long long)(sh + 1023) << 52)
                        : ldexp(v, sh);
+  if constexpr (7 + 8 * (ND - 1) > 51) return __double2ll_rn(t) + bias;
   return __double_as_longlong(t + kRound) - __double_as_longlong(kRound) + bias;
 }
 
@@ -328,20 +332,29 @@ void build_ozaki_planes(Plan& p, cudaStream_t s) {
   else fail(DFJK_ERR_UNSUPPORTED, "mixed precision supports nao <= 12800");
 }
 
+// split_rows_kernel with the build product's digit count of the plan
+static void split_rows(const Plan& p, unsigned nrow, const double* src, int64_t ld, int64_t ncols,
+                       int64_t kp, int* e, int64_t plane, int8_t* planes, int* flag,
+                       cudaStream_t s) {
+  if (build_digits(p) == kOzB64Digits)
+    split_rows_kernel<kOzB64Digits><<<nrow, 256, 0, s>>>(src, ld, ncols, kp, e, plane, planes, flag);
+  else
+    split_rows_kernel<kOzBDigits><<<nrow, 256, 0, s>>>(src, ld, ncols, kp, e, plane, planes, flag);
+  DFJK_LAUNCHED();
+}
+
 void ozaki_prepare_l(Plan& p, cudaStream_t s) {
   p.naux_p16 = (p.naux + 15) / 16 * 16;
   const int64_t plane = p.ldb * p.naux_p16;
-  p.ws_oz_l.ensure((size_t)kOzBDigits * plane);
+  p.ws_oz_l.ensure((size_t)build_digits(p) * plane);
   p.ws_oz_el.ensure((size_t)p.ldb * sizeof(int));
   // L is column-major naux x ldb: column x (contiguous over P) is row x of L^T
   // one flag for every digit split of this build (L and the raw rows),
   // read with the pipeline's error flag by ozaki_check at the end
   p.ws_flag.ensure(sizeof(int));
   DFJK_CUDA(cudaMemsetAsync(p.ws_flag.p, 0, sizeof(int), s));
-  split_rows_kernel<kOzBDigits><<<(unsigned)p.ldb, 256, 0, s>>>(
-      p.d_L.as<double>(), p.naux, p.naux, p.naux_p16, p.ws_oz_el.as<int>(), plane,
-      p.ws_oz_l.as<int8_t>(), p.ws_flag.as<int>());
-  DFJK_LAUNCHED();
+  split_rows(p, (unsigned)p.ldb, p.d_L.as<double>(), p.naux, p.naux, p.naux_p16,
+             p.ws_oz_el.as<int>(), plane, p.ws_oz_l.as<int8_t>(), p.ws_flag.as<int>(), s);
   p.ws_oz_err.ensure(sizeof(int));
   DFJK_CUDA(cudaMemsetAsync(p.ws_oz_err.p, 0, sizeof(int), s));
 }
@@ -361,10 +374,8 @@ void ozaki_split_raw(Plan& p, const double* raw, int64_t nr, int8_t* planes, int
                      int* e, cudaStream_t s) {
   if (nr <= 0) return;
   p.naux_p16 = (p.naux + 15) / 16 * 16;
-  split_rows_kernel<kOzBDigits><<<(unsigned)nr, 256, 0, s>>>(raw, p.naux, p.naux, p.naux_p16, e,
-                                                             plane_stride, planes,
-                                                             p.ws_flag.as<int>());
-  DFJK_LAUNCHED();
+  split_rows(p, (unsigned)nr, raw, p.naux, p.naux, p.naux_p16, e, plane_stride, planes,
+             p.ws_flag.as<int>(), s);
 }
 
 // Bout[r][x] (ld ldb) = sum_P raw[r][P] L[P][x] for nr rows given as digit
@@ -372,8 +383,10 @@ void ozaki_split_raw(Plan& p, const double* raw, int64_t nr, int8_t* planes, int
 void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int* e, int64_t nr,
                  double* Bout, cudaStream_t s) {
   if (nr <= 0) return;
-  constexpr int ND = kOzBDigits;
-  const OzakiShapeInfo sh = ozaki_shape(kOzBuild);
+  const int ND = build_digits(p);
+  const OzakiShape shape = ND == kOzB64Digits ? kOzBuild64 : kOzBuild;
+  const OzakiShapeInfo sh = ozaki_shape(shape);
+  if (sh.digits != ND) fail(DFJK_ERR_INVALID, "build product: digit count of the shape");
   const int bk = sh.box_k;
   const int64_t kp = p.naux_p16;
   OzakiMaps maps;
@@ -401,7 +414,7 @@ void ozaki_bgemm(Plan& p, const int8_t* planes, int64_t plane_stride, const int*
     a.M = (int)mr;
     a.ea = e + m0;
     a.out = Bout + m0 * p.ldb;
-    ozaki_launch(kOzBuild, maps, a, 1, s);
+    ozaki_launch(shape, maps, a, 1, s);
   }
   // checked once per build (ozaki_check)
 }

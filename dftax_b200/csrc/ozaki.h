@@ -9,17 +9,26 @@
 namespace dfjk {
 
 constexpr int kOzKDigits = 4;      // K half transform: 2^-32 of each row's scale
-constexpr int kOzBDigits = 5;      // B = (ij|P) L: 2^-40 (see ozaki.cu)
+constexpr int kOzBDigits = 5;      // B = (ij|P) L, mixed precision: 2^-40 (see ozaki.cu)
+constexpr int kOzB64Digits = 7;    // B = (ij|P) L, float64 plans: 2^-56 of each row's scale
 constexpr int kOzSDigits = 5;      // K = X X^T: 2^-40
-constexpr int kOzMaxDigits = 5;
+constexpr int kOzMaxDigits = 7;
 // longest exact dot product: 5 digits, order 4 sums 2*65*128 + 3*128*128 per k
 constexpr int64_t kOzMaxK = 32640;
+// 7 digits: order 6 sums 2*65*128 + 5*128*128 = 98560 per k, below 2^31 for k <= 21788
+constexpr int64_t kOzMaxK7 = 21788;
 constexpr int64_t kOzSlice = 8192;  // k bytes per slice of the K = X X^T product
 
 // The products and the tile shape each one runs with (ozaki_gemm.cu).
 // kOzHalfWide: the half transform with 96 occupied columns per tile, used when
 // it needs fewer tiles than 80 columns would (each tile streams every B_x plane)
-enum OzakiShape { kOzBuild = 0, kOzHalf = 1, kOzSyrk = 2, kOzHalfWide = 3 };
+// kOzBuild64: the build product of float64 plans, 7 digits on SM pairs
+enum OzakiShape { kOzBuild = 0, kOzHalf = 1, kOzSyrk = 2, kOzHalfWide = 3, kOzBuild64 = 4 };
+
+// digits per value of the build product B = (ij|P) L of a plan
+inline int build_digits(const Plan& p) {
+  return p.opts.precision == DFJK_MIXED ? kOzBDigits : kOzB64Digits;
+}
 struct OzakiShapeInfo {
   int digits, box_k, bn, stages;   // digits per value, k tile bytes, n tile, ring depth
   int box_b;                       // B rows per copy: bn, or bn / 2 on SM pairs

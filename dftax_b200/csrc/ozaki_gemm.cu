@@ -161,12 +161,28 @@ __device__ __forceinline__ double scale_pow2(double x, int e) {
   return ldexp(x, e);
 }
 
+// Past 5 digits the int64 sum would overflow (order 0 times 2^48 for 7
+// digits): orders 0-3 and orders 4.. are summed apart in int64, each below
+// 2^53 and so exact as a float64 (order 0 < 2^28, the others < 2^31), and one
+// FMA joins them with a single rounding.
 template <int ND>
 __device__ __forceinline__ double combine_orders(const uint32_t (&v)[ND][16], int j, int e) {
-  long long s = (int)v[0][j];
+  if constexpr (ND <= 5) {
+    long long s = (int)v[0][j];
 #pragma unroll
-  for (int o = 1; o < ND; ++o) s = s * 256 + (int)v[o][j];
-  return scale_pow2((double)s, e - 14 - 8 * (ND - 1));
+    for (int o = 1; o < ND; ++o) s = s * 256 + (int)v[o][j];
+    return scale_pow2((double)s, e - 14 - 8 * (ND - 1));
+  } else {
+    static_assert(ND <= 8, "the low part holds at most four orders");
+    long long hi = (int)v[0][j];
+#pragma unroll
+    for (int o = 1; o < 4; ++o) hi = hi * 256 + (int)v[o][j];
+    long long lo = (int)v[4][j];
+#pragma unroll
+    for (int o = 5; o < ND; ++o) lo = lo * 256 + (int)v[o][j];
+    constexpr double kLoScale = (double)(1LL << (8 * (ND - 4)));
+    return scale_pow2(fma((double)hi, kLoScale, (double)lo), e - 14 - 8 * (ND - 1));
+  }
 }
 
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int c0, int c1,
@@ -704,6 +720,8 @@ OzakiShapeInfo ozaki_shape(OzakiShape shape) {
     case kOzHalfWide: return {kOzKDigits, 64, 96, 2, 96};
     case kOzBuild: return {kOzBDigits, 64, 96, 4, 48};
     case kOzSyrk: return {kOzSDigits, 64, 96, 3, 96};
+    // 7 orders x 64 columns = 448 of the 512 TMEM columns; three 70 KB stages
+    case kOzBuild64: return {kOzB64Digits, 64, 64, 3, 32};
   }
   fail(DFJK_ERR_INVALID, "unknown int8 GEMM shape %d", (int)shape);
 }
@@ -746,7 +764,7 @@ void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t batches, 
 void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, int grid_z,
                   cudaStream_t s) {
   if (grid_z <= 0 || a.M <= 0 || a.N <= 0) return;
-  static_assert(kOzKDigits == 4 && kOzBDigits == 5 && kOzSDigits == 5,
+  static_assert(kOzKDigits == 4 && kOzBDigits == 5 && kOzSDigits == 5 && kOzB64Digits == 7,
                 "the compiled shapes follow the digit counts");
   switch (shape) {
     case kOzHalf:
@@ -761,6 +779,10 @@ void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, i
     case kOzBuild:
       if (grid_z != 1) fail(DFJK_ERR_INVALID, "the two-SM build product takes one batch");
       launch_pair<5, 64, 96, 4>(maps, a, s);
+      return;
+    case kOzBuild64:
+      if (grid_z != 1) fail(DFJK_ERR_INVALID, "the two-SM build product takes one batch");
+      launch_pair<7, 64, 64, 3>(maps, a, s);
       return;
     case kOzSyrk: launch<5, 64, 96, 3, false>(maps, a, grid_z, s); return;
   }

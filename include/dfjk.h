@@ -38,7 +38,9 @@ typedef enum {
 
 /* Precision of the build and contractions. */
 enum {
-  DFJK_FP64 = 0,  /* float64 integrals, B, J and K                               */
+  DFJK_FP64 = 0,  /* float64 integrals, B, J and K; B = (ij|P) L on int8 tensor
+                     cores with 7 digits per value (2^-56 of each row scale) and
+                     exact int32 accumulation, for naux <= 21788            */
   DFJK_MIXED = 1  /* float64 integrals, metric, stored B and J; the products
                      B = (ij|P) L, X = B_x C and K = X X^T (5, 4 and 5 int8
                      digits per value) on int8 tensor cores with exact int32
