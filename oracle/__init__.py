@@ -19,4 +19,9 @@ Modules:
   df     — ``dftax/ks/terms.py`` (metric pseudo-inverse, DFCoulomb energy,
            RI-K factor and orbital recovery) and ``dftax/energy/hybrid.py``
            (DF-K), with J and K as the analytic gradients of the energy.
+  cpu    — the same 3-center and 2-center integrals compiled (``cpu_df.cpp``,
+           C++ on all host threads) and a full DF build with dftax's J/K
+           contractions: the timed CPU baseline of ``bench.py``, checked
+           against the golden fixtures and against ``md``
+           (``tests/test_oracle_cpu.py``).
 """
