@@ -1,0 +1,129 @@
+"""The oracle's Kohn-Sham pieces (oracle/ks.py) against dftax's own outputs
+(tests/golden/water_scf_ref.npz, made by tests/golden/make_golden_scf.py).
+
+Tolerances: one-electron integrals 1e-13 absolute; grid points 1e-13 and
+weights 1e-13 relative (the Lebedev rules come from SciPy, matched point by
+point to dftax's vendored tables); AO values 1e-14 and gradients 1e-12
+(complex-step on dftax's side); PBE0 eps 1e-14 relative and its derivatives
+1e-7 (rho) and 1e-6 (grad rho) relative: the reference side is a
+Richardson-extrapolated central difference whose round-off, eps |rho e_xc| / h,
+reaches 2e-7 of the derivative at the low-density samples; E_xc 1e-12
+relative; Tr(V_xc Q) against the reference's difference quotient of E_xc along
+Q, 1e-7 relative.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden_basis, load_golden
+
+
+@pytest.fixture(scope="module")
+def scf_golden():
+    return load_golden("water_scf")
+
+
+@pytest.fixture(scope="module")
+def orb(water_golden):
+    return golden_basis(water_golden, "orb")
+
+
+def test_one_electron_matches_reference(scf_golden, orb):
+    from oracle import ks
+
+    g = scf_golden
+    S, T, V = ks.one_electron(orb, g["coords"], g["charges"])
+    assert np.abs(S - g["S"]).max() < 1e-13
+    assert np.abs(T - g["T"]).max() < 1e-13
+    assert np.abs(V - g["V"]).max() < 1e-12
+    assert abs(ks.nuclear_repulsion(g["coords"], g["charges"]) - g["e_nn"]) < 1e-13
+
+
+def _match(a, b):
+    """index of the point of b nearest each point of a"""
+    from scipy.spatial import cKDTree
+
+    d, i = cKDTree(b).query(a)
+    return d, i
+
+
+@pytest.mark.parametrize("tag,spec", [("small", (40, 110)), ("default", (75, 302))])
+def test_becke_grid_matches_reference(scf_golden, tag, spec):
+    from oracle import ks
+
+    g = scf_golden
+    pts, w = ks.becke_grid(list(g["symbols"]), g["coords"], spec[0], spec[1])
+    ref_p, ref_w = g[f"grid_{tag}_coords"], g[f"grid_{tag}_weights"]
+    assert pts.shape == ref_p.shape
+    d, i = _match(ref_p, pts)
+    assert d.max() < 1e-12
+    assert len(np.unique(i)) == len(i)
+    assert np.abs(w[i] - ref_w).max() < 1e-13 * np.abs(ref_w).max()
+
+
+def test_ao_values_and_gradients_match_reference(scf_golden, orb):
+    from oracle import ks
+
+    g = scf_golden
+    pts = g["grid_small_coords"][g["ao_sample_idx"]]
+    val, grad = ks.eval_ao(orb, pts)
+    assert np.abs(val - g["ao_sample"]).max() < 1e-14
+    assert np.abs(grad - g["dao_sample"]).max() < 1e-12
+
+
+def test_pbe0_matches_reference_pointwise(scf_golden):
+    import torch
+
+    from oracle import ks
+
+    g = scf_golden
+    rho = torch.tensor(g["pbe0_rho"], requires_grad=True)
+    grad = torch.tensor(g["pbe0_grad"], requires_grad=True)
+    eps = ks.pbe0_eps(torch, rho, grad)
+    assert np.allclose(eps.detach().numpy(), g["pbe0_eps"], rtol=1e-14, atol=0)
+    (rho * eps).sum().backward()
+    np.testing.assert_allclose(rho.grad.numpy(), g["pbe0_drho"], rtol=1e-7)
+    dg = grad.grad.numpy()
+    scale = np.abs(g["pbe0_dgrad"]).max(axis=1, keepdims=True)
+    assert np.all(np.abs(dg - g["pbe0_dgrad"]) <= 1e-6 * scale)
+
+
+def test_exc_and_vxc_match_reference(scf_golden, orb):
+    from oracle import ks
+
+    g = scf_golden
+    P = 2.0 * g["C"] @ g["C"].T
+    e, vxc = ks.exc_and_vxc(orb, g["grid_small_coords"], g["grid_small_weights"], P)
+    assert abs(e - g["e_xc"]) < 1e-12 * abs(g["e_xc"])
+    for Q, dE in zip(g["dexc_Q"], g["dexc"]):
+        assert abs(np.sum(vxc * Q) - dE) < 1e-7 * abs(dE)
+
+
+def test_scf_converges_to_a_stationary_density(scf_golden, orb, water_golden):
+    """The oracle SCF on the water monomer (golden grid): converged, the
+    commutator at the solution below d_tol, and E(P*) equal to the sum of the
+    reference's own terms at P* (one-electron, DFCoulomb, E_xc, nuclear)."""
+    from oracle import df as odf
+    from oracle import ks
+
+    g = scf_golden
+    aux = golden_basis(water_golden, "aux")
+    from conftest import unpack_tril
+
+    I3 = unpack_tril(water_golden["int3c_tril"], orb.nao)
+    model = ks.KSEnergy(orb, aux, g["coords"], g["charges"], g["grid_small_coords"],
+                        g["grid_small_weights"], I3=I3, vinv=water_golden["vinv"])
+    e, P, eps, C, n_iter, conv = ks.scf(model, 5)
+    assert conv and n_iter < 40
+    # the reference's terms at P*
+    e_ref = (np.sum(P * (g["T"] + g["V"])) + g["e_nn"]
+             + odf.df_energy(I3, water_golden["vinv"], P[None], 0.25)
+             + ks.exc_and_vxc(orb, g["grid_small_coords"], g["grid_small_weights"], P)[0])
+    assert abs(e - e_ref) < 1e-10
+    _, F = model.energy_fock(P)
+    S = g["S"]
+    X = ks.canonical_orthonormalizer(S)
+    assert np.linalg.norm(X.T @ (F @ P @ S - S @ P @ F) @ X) < 1e-6
+    # aufbau: the occupied orbitals lie below the virtual ones (the synthetic
+    # even-tempered basis has no tight O 1s exponents, so E is about -60 Ha)
+    assert eps[4] < 0.0 < eps[5] or eps[4] < eps[5]
