@@ -1,4 +1,4 @@
-"""ctypes bindings of the C ABI declared in ``include/dfjk.h``.
+"""ctypes bindings of the C ABI declared in ``include/dfjk.h`` and ``include/dfscf.h``.
 
 The library ``libdfjk.so`` is built in-tree by ``dftax_b200.build``. There is
 no fallback: if the library is missing or fails to load, every entry point
@@ -27,6 +27,10 @@ EXPORTS = (
     "dfjk_jk_host", "dfjk_energy", "dfjk_eri3c_dense", "dfjk_eri2c_dense", "dfjk_metric_pinv",
     "dfjk_kept_pairs", "dfjk_boys", "dfjk_phase_times", "dfjk_kernel_launches",
     "dfjk_j_noalloc", "dfjk_trim", "dfjk_plan_long_range", "dfjk_energy_rsh",
+    # include/dfscf.h
+    "dfscf_default_options", "dfscf_create", "dfscf_destroy", "dfscf_run", "dfscf_get_result",
+    "dfscf_get_density", "dfscf_get_orbitals", "dfscf_one_electron", "dfscf_xc",
+    "dfscf_energy_fock", "dfjk_becke_partition",
 )
 PHASES = ("metric", "pairs", "eri3c", "bgemm", "j", "khalf", "ksyrk", "kplanes")
 
@@ -60,6 +64,20 @@ class PlanInfo(ctypes.Structure):
                 ("naux_cart", c_int64), ("nshell", c_int64), ("naux_shell", c_int64),
                 ("npair_shell", c_int64), ("nrows", c_int64), ("nfit", c_int64),
                 ("b_bytes", c_int64), ("built", c_int32), ("precision", c_int32)]
+
+
+class ScfOptions(ctypes.Structure):
+    _fields_ = [("hf_coeff", c_double), ("x_scale", c_double), ("c_scale", c_double),
+                ("e_tol", c_double), ("d_tol", c_double), ("lindep", c_double),
+                ("level_shift", c_double), ("rho_thresh", c_double), ("max_iter", c_int32),
+                ("diis_space", c_int32), ("grid_chunk", c_int64)]
+
+
+class ScfResult(ctypes.Structure):
+    _fields_ = [("e_tot", c_double), ("e_one", c_double), ("e_coul", c_double),
+                ("e_xc", c_double), ("e_nn", c_double), ("derr", c_double),
+                ("n_iter", c_int32), ("converged", c_int32), ("nmo", c_int32),
+                ("nocc", c_int32)]
 
 
 _lib = None
@@ -101,6 +119,18 @@ def load(path: str | None = None):
         "dfjk_trim": (c_int, [V]),
         "dfjk_plan_long_range": (c_int, [V, P(c_void_p)]),
         "dfjk_energy_rsh": (c_int, [V, V, c_int32, c_double, c_double, P(c_double), V, V]),
+        "dfscf_default_options": (None, [P(ScfOptions)]),
+        "dfscf_create": (c_int, [V, c_int32, V, V, c_int64, V, V, c_int32, P(ScfOptions),
+                                 P(c_void_p)]),
+        "dfscf_destroy": (c_int, [V]),
+        "dfscf_run": (c_int, [V, V, P(ScfOptions), V]),
+        "dfscf_get_result": (c_int, [V, P(ScfResult)]),
+        "dfscf_get_density": (c_int, [V, V, V]),
+        "dfscf_get_orbitals": (c_int, [V, V, V, V]),
+        "dfscf_one_electron": (c_int, [V, V, V, V, V]),
+        "dfscf_xc": (c_int, [V, V, P(c_double), V, V]),
+        "dfscf_energy_fock": (c_int, [V, V, P(c_double), V, V]),
+        "dfjk_becke_partition": (c_int, [V, V, V, V, c_int64, c_int32, V, V, V, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -117,5 +147,6 @@ def check(status: int, ctx=None):
         raise DfjkError(status, msg)
 
 
-__all__ = ["load", "check", "Basis", "Options", "PlanInfo", "DfjkError", "LibraryNotLoaded",
+__all__ = ["load", "check", "Basis", "Options", "PlanInfo", "ScfOptions", "ScfResult", "DfjkError",
+           "LibraryNotLoaded",
            "EXPORTS", "DFJK_FP64", "DFJK_MIXED", "byref"]

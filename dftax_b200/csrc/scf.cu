@@ -1,0 +1,558 @@
+// Closed-shell Kohn-Sham SCF on the device around a built DF J/K plan
+// (include/dfscf.h). The reference is dftax's _scf_solve (dftax/ks/scf.py:
+// 279-391) with the KS energy of dftax/ks/energy.py:700-723:
+//
+//   E(P) = Tr(P Hcore) + E_J + a_x E_K + E_xc + E_nn,
+//   F(P) = Hcore + J(P) - a_x/2 K(P) + Vxc(P)          (sym(dE/dP), scf.py:42-46)
+//
+// Per iteration, on the density P_k (from aufbau orbitals, so P_k = 2 C_occ
+// C_occ^T and J, K come from the plan's J/K of C_occ with weight 2):
+//   err = X^T (F P S - S P F) X, |err| (scf.py:350-351);
+//   Pulay DIIS over a circular buffer of m Fock and error matrices, the
+//   (m+1) system with unfilled slots masked to the identity and a 1e-10 ridge
+//   on the filled ones (scf.py:245-273), solved on the host;
+//   optional level shift b (S - S P S / 2) (scf.py:367);
+//   X^T F X diagonalized in float64 (cuSOLVER syevd), C = X C', P_{k+1} =
+//   2 C_occ C_occ^T (scf.py:319-327);
+//   E(P_{k+1}) and F(P_{k+1}) together; converged when |E_{k+1} - E_k| < e_tol
+//   and |err_k| < d_tol (scf.py:371).
+// X is the canonical orthonormalizer U s^-1/2 over the overlap eigenvalues
+// above lindep (scf.py:73-90); the guess is the core Hamiltonian's aufbau
+// density (guess.py:605-606) or the caller's P0.
+// Matrices are column-major n x n on the device (the symmetric ones are the
+// same either way); the host synchronizes a few times per iteration for
+// scalars (norms, traces, the DIIS row) and the m x m DIIS solve.
+#include "scf.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace dfjk {
+double energy(Plan& p, const double* P, int nspin, double hf, double hf_lr, double* F,
+              cudaStream_t s);
+}  // namespace dfjk
+
+struct dfscf {
+  dfjk::Plan* p = nullptr;
+  dfjk::Context* c = nullptr;
+  int nao = 0, nocc = 0, natom = 0, nmo = 0, nshell = 0;
+  dfscf_options o{};
+  double e_nn = 0.0;
+  int64_t npts = 0;
+  dfjk::DevBuf atom_xyz, atom_z, pts, wts, out0;
+  dfjk::OrbView ov{};
+  dfjk::DevBuf S, T, V, H, X;
+  dfjk::DevBuf P, C, eps, F, J, K, Vxc, Cocc, wocc;
+  dfjk::DevBuf dF, dE, A1, A2, Fo, work, info, vec;
+  dfjk::XcWork xcw;
+  std::vector<double> B;   // DIIS error overlaps, m x m
+  dfscf_result res{};
+  bool have_orbitals = false;
+};
+
+namespace dfjk {
+namespace {
+
+__global__ void scale_cols_kernel(const double* __restrict__ U, const double* __restrict__ w, int n,
+                                  int first, int nkeep, double* __restrict__ X) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n * nkeep) return;
+  const int64_t r = i % n, k = i / n;
+  X[i] = U[(first + k) * (int64_t)n + r] / sqrt(w[first + k]);
+}
+
+__global__ void fill_upper_kernel(double* __restrict__ A, int n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n * n) return;
+  const int64_t r = i % n, c = i / n;   // column-major (r, c)
+  if (r < c) A[i] = A[c + r * (int64_t)n];
+}
+
+// F = H + J + a K + Vxc (elementwise)
+__global__ void fock_kernel(const double* __restrict__ H, const double* __restrict__ J,
+                            const double* __restrict__ K, const double* __restrict__ Vxc, double a,
+                            int64_t n, double* __restrict__ F) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) F[i] = H[i] + J[i] + (K ? a * K[i] : 0.0) + (Vxc ? Vxc[i] : 0.0);
+}
+
+// y += x
+__global__ void add_inplace_kernel(const double* __restrict__ x, int64_t n, double* y) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
+}
+
+// D = B - B^T (column-major n x n)
+__global__ void antisym_kernel(const double* __restrict__ Bm, int n, double* __restrict__ D) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n * n) return;
+  const int64_t r = i % n, c = i / n;
+  D[i] = Bm[i] - Bm[c + r * (int64_t)n];
+}
+
+unsigned blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+double ddot(Context& c, const double* a, const double* b, int64_t n, cudaStream_t s) {
+  double r = 0.0;
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  DFJK_CUBLAS(cublasDdot(c.cublas, (int)n, a, 1, b, 1, &r));
+  return r;
+}
+
+void gemm(Context& c, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+          double alpha, const double* A, int lda, const double* B, int ldb, double beta, double* C,
+          int ldc, cudaStream_t s) {
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  DFJK_CUBLAS(cublasDgemm(c.cublas, ta, tb, m, n, k, &alpha, A, lda, B, ldb, &beta, C, ldc));
+}
+
+// symmetric eigensolver: A (n x n, overwritten by eigenvectors), w (n)
+void syevd(dfscf& f, double* A, int n, double* w, cudaStream_t s) {
+  Context& c = *f.c;
+  DFJK_CUSOLVER(cusolverDnSetStream(c.cusolver, s));
+  int lwork = 0;
+  DFJK_CUSOLVER(cusolverDnDsyevd_bufferSize(c.cusolver, CUSOLVER_EIG_MODE_VECTOR,
+                                            CUBLAS_FILL_MODE_LOWER, n, A, n, w, &lwork));
+  f.work.ensure((size_t)std::max(lwork, 1) * sizeof(double));
+  f.info.ensure(sizeof(int));
+  DFJK_CUSOLVER(cusolverDnDsyevd(c.cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A,
+                                 n, w, f.work.as<double>(), lwork, f.info.as<int>()));
+  int h = 0;
+  DFJK_CUDA(cudaMemcpyAsync(&h, f.info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  if (h != 0) fail(DFJK_ERR_NUMERIC, "Fock / overlap eigensolver failed (info=%d)", h);
+}
+
+XcParams xc_params(const dfscf& f) {
+  XcParams xp;
+  xp.x_scale = f.o.x_scale;
+  xp.c_scale = f.o.c_scale;
+  xp.rho_thresh = f.o.rho_thresh;
+  return xp;
+}
+
+bool has_xc(const dfscf& f) { return f.npts > 0 && (f.o.x_scale != 0.0 || f.o.c_scale != 0.0); }
+
+// E(P) and F(P) into f.F; J, K through the C_occ of f.C (from_orbitals) or
+// through the plan's density path for a general symmetric P
+double energy_fock(dfscf& f, const double* P, bool from_orbitals, double* Fout, cudaStream_t s) {
+  Context& c = *f.c;
+  const int64_t n = f.nao, nn = n * n;
+  const double hf = f.o.hf_coeff;
+  double e_coul;
+  if (from_orbitals) {
+    // C_occ row-major [nao][nocc] for the plan's J/K; weight 2 per orbital
+    const double one = 1.0, zero = 0.0;
+    DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+    DFJK_CUBLAS(cublasDgeam(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, f.nocc, f.nao, &one, f.C.as<double>(),
+                            f.nao, &zero, f.C.as<double>(), f.nocc, f.Cocc.as<double>(), f.nocc));
+    jk_compute(*f.p, f.Cocc.as<double>(), f.wocc.as<double>(), f.nocc, f.J.as<double>(),
+               hf != 0.0 ? f.K.as<double>() : nullptr, s);
+    e_coul = 0.5 * ddot(c, P, f.J.as<double>(), nn, s);
+    if (hf != 0.0) e_coul -= 0.25 * hf * ddot(c, P, f.K.as<double>(), nn, s);
+    fock_kernel<<<blocks(nn), 256, 0, s>>>(f.H.as<double>(), f.J.as<double>(),
+                                           hf != 0.0 ? f.K.as<double>() : nullptr, nullptr,
+                                           -0.5 * hf, nn, Fout);
+    DFJK_LAUNCHED();
+  } else {
+    // the plan's DFCoulomb energy and gradient (J - a_x/2 K) of any symmetric P
+    e_coul = energy(*f.p, P, 1, hf, 0.0, f.J.as<double>(), s);
+    fock_kernel<<<blocks(nn), 256, 0, s>>>(f.H.as<double>(), f.J.as<double>(), nullptr, nullptr,
+                                           0.0, nn, Fout);
+    DFJK_LAUNCHED();
+  }
+  double e_xc = 0.0;
+  if (has_xc(f)) {
+    e_xc = xc_energy_fock(c, f.ov, f.nshell, f.pts.as<double>(), f.wts.as<double>(), f.npts, P,
+                          f.Vxc.as<double>(), xc_params(f), f.xcw, s);
+    add_inplace_kernel<<<blocks(nn), 256, 0, s>>>(f.Vxc.as<double>(), nn, Fout);
+    DFJK_LAUNCHED();
+  }
+  const double e_one = ddot(c, P, f.H.as<double>(), nn, s);
+  f.res.e_one = e_one;
+  f.res.e_coul = e_coul;
+  f.res.e_xc = e_xc;
+  f.res.e_nn = f.e_nn;
+  return e_one + e_coul + e_xc + f.e_nn;
+}
+
+// orbitals of F into f.C / f.eps and the aufbau density into f.P
+void make_density(dfscf& f, const double* Fm, cudaStream_t s) {
+  Context& c = *f.c;
+  const int n = f.nao, m = f.nmo;
+  // Fo = X^T F X
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, m, n, 1.0, Fm, n, f.X.as<double>(), n, 0.0, f.A1.as<double>(),
+       n, s);
+  gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, 1.0, f.X.as<double>(), n, f.A1.as<double>(), n, 0.0,
+       f.Fo.as<double>(), m, s);
+  syevd(f, f.Fo.as<double>(), m, f.eps.as<double>(), s);
+  // C = X C'
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, 1.0, f.X.as<double>(), n, f.Fo.as<double>(), m, 0.0,
+       f.C.as<double>(), n, s);
+  // P = 2 C_occ C_occ^T (lower by SYRK, then mirrored)
+  const double two = 2.0, zero = 0.0;
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, f.nocc, &two,
+                          f.C.as<double>(), n, &zero, f.P.as<double>(), n));
+  fill_upper_kernel<<<blocks((int64_t)n * n), 256, 0, s>>>(f.P.as<double>(), n);
+  DFJK_LAUNCHED();
+  f.have_orbitals = true;
+}
+
+// err = X^T (F P S - S P F) X into f.Fo's slot of dE; returns |err|
+double commutator(dfscf& f, const double* Fm, const double* Pm, double* err, cudaStream_t s) {
+  Context& c = *f.c;
+  const int n = f.nao, m = f.nmo;
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, Fm, n, Pm, n, 0.0, f.A1.as<double>(), n, s);
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, f.A1.as<double>(), n, f.S.as<double>(), n, 0.0,
+       f.A2.as<double>(), n, s);
+  antisym_kernel<<<blocks((int64_t)n * n), 256, 0, s>>>(f.A2.as<double>(), n, f.A1.as<double>());
+  DFJK_LAUNCHED();
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, m, n, 1.0, f.A1.as<double>(), n, f.X.as<double>(), n, 0.0,
+       f.A2.as<double>(), n, s);
+  gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, 1.0, f.X.as<double>(), n, f.A2.as<double>(), n, 0.0, err,
+       m, s);
+  double r = 0.0;
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  DFJK_CUBLAS(cublasDnrm2(c.cublas, m * m, err, 1, &r));
+  return r;
+}
+
+// DIIS coefficients of the filled slots (scf.py:245-273), host
+std::vector<double> diis_solve(const std::vector<double>& Bm, int count, int m) {
+  const int N = m + 1;
+  std::vector<double> A((size_t)N * N, 0.0), rhs(N, 0.0);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) {
+      const bool v = i < count && j < count;
+      A[(size_t)i * N + j] = v ? Bm[(size_t)i * m + j] : (i == j ? 1.0 : 0.0);
+    }
+  for (int i = 0; i < count; ++i) A[(size_t)i * N + i] += 1e-10;
+  for (int i = 0; i < m; ++i) {
+    const double b = i < count ? -1.0 : 0.0;
+    A[(size_t)i * N + m] = b;
+    A[(size_t)m * N + i] = b;
+  }
+  rhs[m] = -1.0;
+  // Gaussian elimination with partial pivoting
+  std::vector<int> piv(N);
+  for (int k = 0; k < N; ++k) {
+    int p = k;
+    for (int i = k + 1; i < N; ++i)
+      if (std::fabs(A[(size_t)i * N + k]) > std::fabs(A[(size_t)p * N + k])) p = i;
+    if (A[(size_t)p * N + k] == 0.0) fail(DFJK_ERR_NUMERIC, "singular DIIS system");
+    if (p != k) {
+      for (int j = 0; j < N; ++j) std::swap(A[(size_t)k * N + j], A[(size_t)p * N + j]);
+      std::swap(rhs[k], rhs[p]);
+    }
+    for (int i = k + 1; i < N; ++i) {
+      const double l = A[(size_t)i * N + k] / A[(size_t)k * N + k];
+      if (l == 0.0) continue;
+      for (int j = k; j < N; ++j) A[(size_t)i * N + j] -= l * A[(size_t)k * N + j];
+      rhs[i] -= l * rhs[k];
+    }
+  }
+  std::vector<double> x(N);
+  for (int i = N - 1; i >= 0; --i) {
+    double v = rhs[i];
+    for (int j = i + 1; j < N; ++j) v -= A[(size_t)i * N + j] * x[j];
+    x[i] = v / A[(size_t)i * N + i];
+  }
+  x.resize(m);
+  return x;
+}
+
+void run(dfscf& f, const double* P0, cudaStream_t s) {
+  Context& c = *f.c;
+  const int n = f.nao, m = f.nmo, md = f.o.diis_space;
+  const int64_t nn = (int64_t)n * n, mm = (int64_t)m * m;
+  f.res = dfscf_result{};
+  f.res.nmo = f.nmo;
+  f.res.nocc = f.nocc;
+  bool orbitals;
+  if (P0) {
+    DFJK_CUDA(cudaMemcpyAsync(f.P.p, P0, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    orbitals = false;
+  } else {
+    make_density(f, f.H.as<double>(), s);   // core-Hamiltonian guess
+    orbitals = true;
+  }
+  double e_prev = energy_fock(f, f.P.as<double>(), orbitals, f.F.as<double>(), s);
+  f.B.assign((size_t)md * md, 0.0);
+  int it = 0;
+  bool converged = false;
+  double derr = INFINITY;
+  while (it < f.o.max_iter && !converged) {
+    const int slot = it % md;
+    double* dFs = f.dF.as<double>() + slot * nn;
+    double* dEs = f.dE.as<double>() + slot * mm;
+    derr = commutator(f, f.F.as<double>(), f.P.as<double>(), dEs, s);
+    DFJK_CUDA(cudaMemcpyAsync(dFs, f.F.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    // the new row of error overlaps: B[slot][j] = <err_slot, err_j>
+    const int count = std::min(it + 1, md);
+    std::vector<double> row(md, 0.0);
+    for (int j = 0; j < count; ++j)
+      row[j] = ddot(c, dEs, f.dE.as<double>() + j * mm, mm, s);
+    for (int j = 0; j < count; ++j) {
+      f.B[(size_t)slot * md + j] = row[j];
+      f.B[(size_t)j * md + slot] = row[j];
+    }
+    std::vector<double> coef = diis_solve(f.B, count, md);
+    // F_ext = sum_i c_i F_i
+    f.vec.ensure((size_t)md * sizeof(double));
+    DFJK_CUDA(cudaMemcpyAsync(f.vec.p, coef.data(), md * sizeof(double), cudaMemcpyHostToDevice, s));
+    {
+      const double one = 1.0, zero = 0.0;
+      DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+      DFJK_CUBLAS(cublasDgemv(c.cublas, CUBLAS_OP_N, (int)nn, md, &one, f.dF.as<double>(), (int)nn,
+                              f.vec.as<double>(), 1, &zero, f.A2.as<double>(), 1));
+    }
+    double* Fext = f.A2.as<double>();
+    if (f.o.level_shift != 0.0) {
+      // F_ext + b (S - S P S / 2)
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, f.S.as<double>(), n, f.P.as<double>(), n, 0.0,
+           f.A1.as<double>(), n, s);
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, -0.5 * f.o.level_shift, f.A1.as<double>(), n,
+           f.S.as<double>(), n, 1.0, Fext, n, s);
+      const double b = f.o.level_shift;
+      DFJK_CUBLAS(cublasDaxpy(c.cublas, (int)nn, &b, f.S.as<double>(), 1, Fext, 1));
+    }
+    // the DIIS Fock moves to the dedicated buffer before make_density reuses A1/A2
+    DFJK_CUDA(cudaMemcpyAsync(f.Vxc.p, Fext, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    make_density(f, f.Vxc.as<double>(), s);
+    const double e = energy_fock(f, f.P.as<double>(), true, f.F.as<double>(), s);
+    converged = std::fabs(e - e_prev) < f.o.e_tol && derr < f.o.d_tol;
+    e_prev = e;
+    ++it;
+  }
+  f.res.e_tot = e_prev;
+  f.res.derr = derr;
+  f.res.n_iter = it;
+  f.res.converged = converged ? 1 : 0;
+}
+
+}  // namespace
+}  // namespace dfjk
+
+using namespace dfjk;
+
+extern "C" {
+
+void dfscf_default_options(dfscf_options* o) {
+  if (!o) return;
+  *o = dfscf_options{};
+  o->hf_coeff = 0.25;
+  o->x_scale = 0.75;
+  o->c_scale = 1.0;
+  o->e_tol = 1e-8;
+  o->d_tol = 1e-6;
+  o->lindep = 1e-7;
+  o->level_shift = 0.0;
+  o->rho_thresh = 1e-10;
+  o->max_iter = 128;
+  o->diis_space = 8;
+  o->grid_chunk = 0;
+}
+
+dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
+                         const double* atom_charge, int64_t npoint, const double* grid_xyz,
+                         const double* grid_w, int32_t nocc, const dfscf_options* opts,
+                         dfscf** out) {
+  if (!pl || !out) return DFJK_ERR_INVALID;
+  *out = nullptr;
+  dfscf* f = new (std::nothrow) dfscf;
+  if (!f) return DFJK_ERR_MEMORY;
+  Context* c = pl->p.ctx;
+  dfjk_status st = guard(c, [&] {
+    Plan& p = pl->p;
+    if (!p.built) fail(DFJK_ERR_STATE, "dfscf_create before dfjk_build");
+    if (p.lr) fail(DFJK_ERR_UNSUPPORTED, "the SCF does not take range-separated plans");
+    if (natom <= 0 || !atom_xyz || !atom_charge) fail(DFJK_ERR_INVALID, "no atoms");
+    if (npoint < 0 || (npoint > 0 && (!grid_xyz || !grid_w))) fail(DFJK_ERR_INVALID, "bad grid");
+    if (nocc <= 0 || nocc > p.nao) fail(DFJK_ERR_INVALID, "nocc=%d for nao=%d", nocc, p.nao);
+    DFJK_CUDA(cudaSetDevice(c->device));
+    f->p = &p;
+    f->c = c;
+    if (opts) f->o = *opts;
+    else dfscf_default_options(&f->o);
+    if (f->o.diis_space < 1 || f->o.max_iter < 0) fail(DFJK_ERR_INVALID, "invalid SCF options");
+    for (int64_t i = 0; i < 3 * (int64_t)natom; ++i)
+      if (!std::isfinite(atom_xyz[i])) fail(DFJK_ERR_NUMERIC, "non-finite atom coordinate");
+    for (int64_t i = 0; i < 3 * npoint; ++i)
+      if (!std::isfinite(grid_xyz[i])) fail(DFJK_ERR_NUMERIC, "non-finite grid point");
+    f->nao = p.nao;
+    f->nocc = nocc;
+    f->natom = natom;
+    f->npts = npoint;
+    f->nshell = p.orb.n;
+    f->xcw.chunk = f->o.grid_chunk > 0 ? (f->o.grid_chunk + 255) / 256 * 256 : 0;
+    upload(f->atom_xyz, std::vector<double>(atom_xyz, atom_xyz + 3 * natom));
+    upload(f->atom_z, std::vector<double>(atom_charge, atom_charge + natom));
+    if (npoint > 0) {
+      upload(f->pts, std::vector<double>(grid_xyz, grid_xyz + 3 * npoint));
+      upload(f->wts, std::vector<double>(grid_w, grid_w + npoint));
+    }
+    double enn = 0.0;
+    for (int a = 0; a < natom; ++a)
+      for (int b = 0; b < a; ++b) {
+        const double dx = atom_xyz[3 * a] - atom_xyz[3 * b], dy = atom_xyz[3 * a + 1] - atom_xyz[3 * b + 1],
+                     dz = atom_xyz[3 * a + 2] - atom_xyz[3 * b + 2];
+        enn += atom_charge[a] * atom_charge[b] / std::sqrt(dx * dx + dy * dy + dz * dz);
+      }
+    f->e_nn = enn;
+    // orbital shells as the AO and one-electron kernels read them
+    upload(f->out0, p.orb.out0);
+    OrbView& ov = f->ov;
+    ov.sh = ShellView{p.orb.d_l.as<int>(), p.orb.d_nprim.as<int>(), p.orb.d_prim0.as<int>(),
+                      p.orb.d_cen.as<double>(), p.orb.d_pexp.as<double>(), p.orb.d_pcoef.as<double>()};
+    ov.out0 = f->out0.as<int>();
+    ov.c2s = p.c2s_orb.dev.as<double>();
+    for (int l = 0; l < 8; ++l) {
+      ov.c2s_off[l] = p.c2s_orb.off[l];
+      ov.nout[l] = p.orb.spherical ? 2 * l + 1 : ncart(l);
+    }
+    ov.nao = p.nao;
+    const int64_t n = p.nao, nn = n * n;
+    for (DevBuf* b : {&f->S, &f->T, &f->V, &f->H, &f->P, &f->F, &f->J, &f->K, &f->Vxc, &f->A1, &f->A2})
+      b->alloc(nn * sizeof(double));
+    cudaStream_t s = nullptr;
+    launch_one_electron(*c, ov, f->nshell, p.orb.l, natom, f->atom_xyz.as<double>(),
+                        f->atom_z.as<double>(), f->S.as<double>(), f->T.as<double>(),
+                        f->V.as<double>(), s);
+    DFJK_CUBLAS(cublasSetStream(c->cublas, s));
+    const double one = 1.0;
+    DFJK_CUBLAS(cublasDgeam(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)n, &one,
+                            f->T.as<double>(), (int)n, &one, f->V.as<double>(), (int)n,
+                            f->H.as<double>(), (int)n));
+    check_finite(p, f->H.as<double>(), nn, s, "the one-electron integrals");
+    // canonical orthonormalizer X = U s^-1/2 over s > lindep
+    DFJK_CUDA(cudaMemcpyAsync(f->A1.p, f->S.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    DevBuf w;
+    w.alloc(n * sizeof(double));
+    syevd(*f, f->A1.as<double>(), (int)n, w.as<double>(), s);
+    std::vector<double> hw(n);
+    DFJK_CUDA(cudaMemcpy(hw.data(), w.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    int first = 0;
+    while (first < n && !(hw[first] > f->o.lindep)) ++first;
+    f->nmo = (int)(n - first);
+    if (f->nmo < nocc) fail(DFJK_ERR_NUMERIC, "only %d orbitals kept for %d occupied", f->nmo, nocc);
+    const int64_t m = f->nmo;
+    f->X.alloc(n * m * sizeof(double));
+    scale_cols_kernel<<<blocks(n * m), 256, 0, s>>>(f->A1.as<double>(), w.as<double>(), (int)n,
+                                                    first, (int)m, f->X.as<double>());
+    DFJK_LAUNCHED();
+    f->C.alloc(n * m * sizeof(double));
+    f->eps.alloc(m * sizeof(double));
+    f->Fo.alloc(m * m * sizeof(double));
+    f->Cocc.alloc(n * nocc * sizeof(double));
+    upload(f->wocc, std::vector<double>(nocc, 2.0));
+    f->dF.alloc((size_t)f->o.diis_space * nn * sizeof(double));
+    f->dE.alloc((size_t)f->o.diis_space * m * m * sizeof(double));
+    DFJK_CUDA(cudaMemsetAsync(f->dE.p, 0, (size_t)f->o.diis_space * m * m * sizeof(double), s));
+    DFJK_CUDA(cudaStreamSynchronize(s));
+  });
+  if (st != DFJK_OK) {
+    delete f;
+    return st;
+  }
+  *out = f;
+  return DFJK_OK;
+}
+
+dfjk_status dfscf_destroy(dfscf* f) {
+  if (!f) return DFJK_OK;
+  cudaSetDevice(f->c->device);
+  cudaDeviceSynchronize();
+  delete f;
+  return DFJK_OK;
+}
+
+dfjk_status dfscf_run(dfscf* f, const double* P0, const dfscf_options* ro, void* stream) {
+  if (!f) return DFJK_ERR_INVALID;
+  return guard(f->c, [&] {
+    if (ro) {
+      if (ro->max_iter < 0) fail(DFJK_ERR_INVALID, "max_iter=%d", ro->max_iter);
+      f->o.max_iter = ro->max_iter;
+      f->o.e_tol = ro->e_tol;
+      f->o.d_tol = ro->d_tol;
+      f->o.level_shift = ro->level_shift;
+    }
+    DFJK_CUDA(cudaSetDevice(f->c->device));
+    run(*f, P0, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfjk_status dfscf_get_result(const dfscf* f, dfscf_result* r) {
+  if (!f || !r) return DFJK_ERR_INVALID;
+  *r = f->res;
+  return DFJK_OK;
+}
+
+dfjk_status dfscf_get_density(dfscf* f, double* P, void* stream) {
+  if (!f) return DFJK_ERR_INVALID;
+  return guard(f->c, [&] {
+    if (P)
+      DFJK_CUDA(cudaMemcpyAsync(P, f->P.p, (size_t)f->nao * f->nao * sizeof(double),
+                                cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
+  });
+}
+
+dfjk_status dfscf_get_orbitals(dfscf* f, double* eps, double* C, void* stream) {
+  if (!f) return DFJK_ERR_INVALID;
+  return guard(f->c, [&] {
+    if (!f->have_orbitals) fail(DFJK_ERR_STATE, "no orbitals before dfscf_run");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (eps)
+      DFJK_CUDA(cudaMemcpyAsync(eps, f->eps.p, (size_t)f->nmo * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s));
+    if (C)
+      DFJK_CUDA(cudaMemcpyAsync(C, f->C.p, (size_t)f->nao * f->nmo * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s));
+  });
+}
+
+dfjk_status dfscf_one_electron(dfscf* f, double* S, double* T, double* V, void* stream) {
+  if (!f) return DFJK_ERR_INVALID;
+  return guard(f->c, [&] {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t b = (size_t)f->nao * f->nao * sizeof(double);
+    if (S) DFJK_CUDA(cudaMemcpyAsync(S, f->S.p, b, cudaMemcpyDeviceToDevice, s));
+    if (T) DFJK_CUDA(cudaMemcpyAsync(T, f->T.p, b, cudaMemcpyDeviceToDevice, s));
+    if (V) DFJK_CUDA(cudaMemcpyAsync(V, f->V.p, b, cudaMemcpyDeviceToDevice, s));
+  });
+}
+
+dfjk_status dfscf_xc(dfscf* f, const double* P, double* exc, double* Vxc, void* stream) {
+  if (!f || !P || !exc) return DFJK_ERR_INVALID;
+  return guard(f->c, [&] {
+    DFJK_CUDA(cudaSetDevice(f->c->device));
+    *exc = xc_energy_fock(*f->c, f->ov, f->nshell, f->pts.as<double>(), f->wts.as<double>(), f->npts,
+                          P, Vxc, xc_params(*f), f->xcw, static_cast<cudaStream_t>(stream));
+  });
+}
+
+dfjk_status dfscf_energy_fock(dfscf* f, const double* P, double* e, double* F, void* stream) {
+  if (!f || !P || !e) return DFJK_ERR_INVALID;
+  return guard(f->c, [&] {
+    DFJK_CUDA(cudaSetDevice(f->c->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    *e = energy_fock(*f, P, false, F ? F : f->A2.as<double>(), s);
+    DFJK_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+dfjk_status dfjk_becke_partition(dfjk_ctx* h, const double* pts, const int32_t* owner,
+                                 const double* raw, int64_t n, int32_t natom,
+                                 const double* atom_xyz, const double* bragg, double* w,
+                                 void* stream) {
+  if (!h) return DFJK_ERR_INVALID;
+  return guard(&h->c, [&] {
+    if (n < 0 || natom <= 0 || !atom_xyz || !bragg) fail(DFJK_ERR_INVALID, "bad partition input");
+    if (n > 0 && (!pts || !owner || !raw || !w)) fail(DFJK_ERR_INVALID, "null grid array");
+    DFJK_CUDA(cudaSetDevice(h->c.device));
+    launch_becke_partition(pts, owner, raw, n, atom_xyz, bragg, natom, w,
+                           static_cast<cudaStream_t>(stream));
+  });
+}
+
+}  // extern "C"

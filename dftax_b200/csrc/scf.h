@@ -1,0 +1,53 @@
+// Internal declarations of the Kohn-Sham SCF around the DF J/K plan (scf.cu,
+// onee.cu, xc.cu). Not part of the C ABI (include/dfscf.h).
+#pragma once
+
+#include "internal.h"
+#include "../../include/dfscf.h"
+
+namespace dfjk {
+
+// Device view of the orbital shells for the one-electron and AO kernels.
+struct OrbView {
+  ShellView sh;
+  const int* out0;      // first spherical (or cartesian) function of each shell
+  const double* c2s;    // transformation blocks, one per l (ncart(l) x nout(l), row-major)
+  int c2s_off[8];       // offset of l's block in c2s
+  int nout[8];          // functions per shell of each l (2l+1, or ncart(l) without cart2sph)
+  int nao;
+};
+
+// One-electron integrals (onee.cu): S, T and V = -sum_C Z_C <a|1/|r-C||b> as
+// nao x nao matrices (symmetric, both triangles written), for the shell pairs
+// of the orbital basis.
+void launch_one_electron(const Context& c, const OrbView& ov, int nshell, const std::vector<int>& l,
+                         int natom, const double* atom_xyz, const double* atom_z, double* S,
+                         double* T, double* V, cudaStream_t s);
+
+// XC on a point grid (xc.cu)
+struct XcWork {
+  int64_t chunk = 0;            // points per chunk
+  DevBuf phi, dphi, X, W;       // [nao][chunk] AO values, 3 gradients, Phi P, weighted AO
+  DevBuf vr, vg, ered;          // per point: v_rho, v_grad (3), energy partials per block
+};
+
+struct XcParams {
+  double x_scale = 0.75;        // PBE exchange share (PBE0)
+  double c_scale = 1.0;         // PBE correlation share
+  double rho_thresh = 1e-10;    // points at or below this density are left out
+};
+
+// E_xc of the closed-shell density P (nao x nao, symmetric, device) and, when
+// Vxc != nullptr, its P-gradient symmetrized (device, nao x nao), over the grid
+// points pts [n][3] with weights w [n] (device). Uses the context's cuBLAS
+// handle on stream s. Returns E_xc (host synchronizing).
+double xc_energy_fock(const Context& c, const OrbView& ov, int nshell, const double* pts,
+                      const double* w, int64_t npts, const double* P, double* Vxc,
+                      const XcParams& xp, XcWork& ws, cudaStream_t s);
+
+// Becke cell weights: w[i] = raw[i] * P_owner(i) / sum_A P_A at point i
+void launch_becke_partition(const double* pts, const int* owner, const double* raw, int64_t n,
+                            const double* atom_xyz, const double* bragg, int natom, double* w,
+                            cudaStream_t s);
+
+}  // namespace dfjk

@@ -1,0 +1,426 @@
+// Exchange-correlation energy and Fock matrix of a closed-shell density on a
+// point grid, and the Becke partition of an atom-centered grid.
+//
+// Per chunk of G points (dftax/ks/terms.py:776-828, GridXC; energy/grid.py:10-45):
+//   Phi[mu][g], dPhi[x][mu][g]   AO values and gradients (ao_kernel: one thread
+//                                per point and shell, points fastest, so the
+//                                stores of a warp are contiguous), as
+//                                dftax/energy/gto.py:371-412 evaluates them;
+//   X = Phi P                    cuBLAS DGEMM;
+//   rho_g = sum_mu X Phi, grad rho_g = 2 sum_mu X dPhi        (rho_kernel);
+//   e_g = w rho eps_xc(rho, grad rho) and its derivatives v_rho, v_grad by
+//   forward-mode dual numbers over the same expression as dftax's PBE
+//   (xc.py:87-252, PBE0 :584-601; points with rho <= 1e-10 contribute nothing,
+//   as the double-where of grid.py:31-44 makes them);
+//   W = v_rho/2 Phi + v_grad . dPhi, V += Phi^T W               (cuBLAS DGEMM);
+// and at the end Vxc = V + V^T, the symmetrized P-gradient of E_xc
+// (scf.py:42-46). The energy is summed per block in a fixed order and then
+// over blocks on the host, so it is reproducible.
+#include "scf.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace dfjk {
+namespace {
+
+constexpr int kAoThreads = 128;
+constexpr int kPtThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Becke partition
+// ---------------------------------------------------------------------------
+
+// one thread per point; the point's distances to the atoms in shared memory
+__global__ void becke_kernel(const double* __restrict__ pts, const int* __restrict__ owner,
+                             const double* __restrict__ raw, int64_t n,
+                             const double* __restrict__ xyz, const double* __restrict__ inv_rab,
+                             const double* __restrict__ aab, int natom, double* __restrict__ w) {
+  extern __shared__ double sr[];   // [natom][blockDim.x]
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int lt = threadIdx.x, nt = blockDim.x;
+  if (i >= n) return;
+  const double px = pts[3 * i], py = pts[3 * i + 1], pz = pts[3 * i + 2];
+  for (int a = 0; a < natom; ++a) {
+    const double dx = px - xyz[3 * a], dy = py - xyz[3 * a + 1], dz = pz - xyz[3 * a + 2];
+    sr[a * nt + lt] = sqrt(dx * dx + dy * dy + dz * dz + 1e-30);
+  }
+  const int own = owner[i];
+  double total = 0.0, mine = 0.0;
+  for (int a = 0; a < natom; ++a) {
+    const double ra = sr[a * nt + lt];
+    double cell = 1.0;
+    for (int b = 0; b < natom; ++b) {
+      if (b == a) continue;
+      const double mu = (ra - sr[b * nt + lt]) * inv_rab[a * natom + b];
+      double f = mu + aab[a * natom + b] * (1.0 - mu * mu);
+      f = 1.5 * f - 0.5 * f * f * f;
+      f = 1.5 * f - 0.5 * f * f * f;
+      f = 1.5 * f - 0.5 * f * f * f;
+      cell *= 0.5 * (1.0 - f);
+    }
+    total += cell;
+    if (a == own) mine = cell;
+  }
+  w[i] = raw[i] * mine / total;
+}
+
+// ---------------------------------------------------------------------------
+// AO values and gradients
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double ipow(double x, int n) {
+  double r = 1.0;
+  for (int k = 0; k < n; ++k) r *= x;
+  return r;
+}
+
+// Phi[mu][g] (ld G), dPhi[x][mu][g]; grid (ceil(ng / 128), nshell)
+__global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const double* __restrict__ pts,
+                                                        int64_t g0, int64_t ng, int64_t G,
+                                                        double* __restrict__ phi,
+                                                        double* __restrict__ dphi) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (g >= G) return;
+  const ShellView& sh = ov.sh;
+  const int l = sh.l[s], nc = (l + 1) * (l + 2) / 2, nout = ov.nout[l];
+  const int64_t mu0 = ov.out0[s];
+  const int64_t plane = (int64_t)ov.nao * G;
+  double val[10] = {}, gx[10] = {}, gy[10] = {}, gz[10] = {};
+  if (g < ng) {
+    const double* p = pts + 3 * (g0 + g);
+    const double dx = p[0] - sh.cen[3 * s], dy = p[1] - sh.cen[3 * s + 1],
+                 dz = p[2] - sh.cen[3 * s + 2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    double rad = 0.0, drad = 0.0;
+    for (int k = 0; k < sh.nprim[s]; ++k) {
+      const double a = sh.pexp[sh.prim0[s] + k], c = sh.pcoef[sh.prim0[s] + k];
+      const double e = c * exp(-a * r2);
+      rad += e;
+      drad += -2.0 * a * e;
+    }
+    int k = 0;
+    for (int lx = l; lx >= 0; --lx)
+      for (int ly = l - lx; ly >= 0; --ly, ++k) {
+        const int lz = l - lx - ly;
+        const double px_ = ipow(dx, lx), py_ = ipow(dy, ly), pz_ = ipow(dz, lz);
+        const double ang = px_ * py_ * pz_;
+        val[k] = ang * rad;
+        const double dpx = lx > 0 ? lx * ipow(dx, lx - 1) : 0.0;
+        const double dpy = ly > 0 ? ly * ipow(dy, ly - 1) : 0.0;
+        const double dpz = lz > 0 ? lz * ipow(dz, lz - 1) : 0.0;
+        gx[k] = dpx * py_ * pz_ * rad + ang * drad * dx;
+        gy[k] = px_ * dpy * pz_ * rad + ang * drad * dy;
+        gz[k] = px_ * py_ * dpz * rad + ang * drad * dz;
+      }
+  }
+  const double* T = ov.c2s + ov.c2s_off[l];
+  for (int m = 0; m < nout; ++m) {
+    double v = 0.0, a = 0.0, b = 0.0, c = 0.0;
+    for (int q = 0; q < nc; ++q) {
+      const double t = T[q * nout + m];
+      v += val[q] * t;
+      a += gx[q] * t;
+      b += gy[q] * t;
+      c += gz[q] * t;
+    }
+    const int64_t o = (mu0 + m) * G + g;
+    phi[o] = v;
+    dphi[o] = a;
+    dphi[plane + o] = b;
+    dphi[2 * plane + o] = c;
+  }
+}
+
+// rho[g] = sum_mu X Phi, grad[x][g] = 2 sum_mu X dPhi_x
+__global__ void rho_kernel(const double* __restrict__ X, const double* __restrict__ phi,
+                           const double* __restrict__ dphi, int nao, int64_t G, int64_t ng,
+                           double* __restrict__ rho, double* __restrict__ grad) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  const int64_t plane = (int64_t)nao * G;
+  double r = 0.0, a = 0.0, b = 0.0, c = 0.0;
+  for (int mu = 0; mu < nao; ++mu) {
+    const int64_t o = (int64_t)mu * G + g;
+    const double x = X[o];
+    r += x * phi[o];
+    a += x * dphi[o];
+    b += x * dphi[plane + o];
+    c += x * dphi[2 * plane + o];
+  }
+  rho[g] = r;
+  grad[g] = 2.0 * a;
+  grad[G + g] = 2.0 * b;
+  grad[2 * G + g] = 2.0 * c;
+}
+
+// ---------------------------------------------------------------------------
+// PBE by forward-mode dual numbers: value and d/d(rho, gx, gy, gz)
+// ---------------------------------------------------------------------------
+
+struct D4 {
+  double v, d[4];
+};
+__device__ __forceinline__ D4 dc(double c) { return {c, {0.0, 0.0, 0.0, 0.0}}; }
+__device__ __forceinline__ D4 operator+(D4 a, D4 b) {
+  return {a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2], a.d[3] + b.d[3]}};
+}
+__device__ __forceinline__ D4 operator*(D4 a, D4 b) {
+  D4 r;
+  r.v = a.v * b.v;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return r;
+}
+__device__ __forceinline__ D4 operator/(D4 a, D4 b) {
+  D4 r;
+  r.v = a.v / b.v;
+  const double ib2 = 1.0 / (b.v * b.v);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r.d[k] = (a.d[k] * b.v - a.v * b.d[k]) * ib2;
+  return r;
+}
+__device__ __forceinline__ D4 operator+(D4 a, double c) { a.v += c; return a; }
+__device__ __forceinline__ D4 operator+(double c, D4 a) { a.v += c; return a; }
+__device__ __forceinline__ D4 operator-(double c, D4 a) {
+  return {c - a.v, {-a.d[0], -a.d[1], -a.d[2], -a.d[3]}};
+}
+__device__ __forceinline__ D4 operator*(D4 a, double c) {
+  return {a.v * c, {a.d[0] * c, a.d[1] * c, a.d[2] * c, a.d[3] * c}};
+}
+__device__ __forceinline__ D4 operator*(double c, D4 a) { return a * c; }
+__device__ __forceinline__ D4 operator/(D4 a, double c) { return a * (1.0 / c); }
+__device__ __forceinline__ D4 operator/(double c, D4 a) { return dc(c) / a; }
+__device__ __forceinline__ D4 dscale(D4 a, double f) {   // chain rule with df/dx = f
+  D4 r;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] * f;
+  return r;
+}
+__device__ __forceinline__ D4 dsqrt(D4 a) {
+  D4 r = dscale(a, 0.5 / sqrt(a.v));
+  r.v = sqrt(a.v);
+  return r;
+}
+__device__ __forceinline__ D4 dpow(D4 a, double e) {
+  D4 r = dscale(a, e * pow(a.v, e - 1.0));
+  r.v = pow(a.v, e);
+  return r;
+}
+__device__ __forceinline__ D4 dlog1p(D4 a) {
+  D4 r = dscale(a, 1.0 / (1.0 + a.v));
+  r.v = log1p(a.v);
+  return r;
+}
+__device__ __forceinline__ D4 dexpm1(D4 a) {
+  D4 r = dscale(a, exp(a.v));
+  r.v = expm1(a.v);
+  return r;
+}
+// jnp.clip(x, lo): the bound itself (derivative 0) below lo
+__device__ __forceinline__ D4 dclip(D4 a, double lo) { return a.v < lo ? dc(lo) : a; }
+
+// eps_xc per particle of x_scale PBE exchange + c_scale PBE correlation,
+// unpolarized (xc.py: PBEExchange._unpolarized, PBECorrelation with zeta = 0)
+__device__ D4 pbe_eps(D4 rho, D4 gx, D4 gy, D4 gz, double xs, double cs) {
+  constexpr double pi = 3.141592653589793;
+  constexpr double third = 1.0 / 3.0;
+  // exchange
+  const D4 ax = gx + 1e-30, ay = gy + 1e-30, az = gz + 1e-30;
+  const D4 gnorm = dsqrt(ax * ax + ay * ay + az * az);
+  const D4 kF = dpow(3 * pi * pi * rho + 1e-30, third);
+  const D4 s = gnorm / dclip(2 * kF * rho, 1e-30);
+  const double kappa = 0.804, mu = 0.2195149727645171;
+  const D4 ex_unif = -3 * kF / (4 * pi);
+  const D4 fx = 1 + kappa - kappa / (1 + mu * s * s / kappa);
+  const D4 ex = ex_unif * fx;
+  // correlation: PW92 paramagnetic channel + PBE H with phi = 1
+  const double gamma = (1.0 - 0.6931471805599453) / (pi * pi);
+  const double beta = 0.06672455060314922;
+  const double A = 0.0310907, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+  const D4 rt = dclip(rho, 1e-20);
+  const D4 rs = dpow(3 / (4 * pi * rt) + 1e-20, third);
+  const D4 rss = dsqrt(rs);
+  const D4 den = 2.0 * A * (b1 * rss + b2 * rs + b3 * rs * rss + b4 * rs * rs);
+  const D4 eps_pw = -2.0 * A * (1.0 + a1 * rs) * dlog1p(1.0 / dclip(den, 1e-20));
+  const D4 kf = dpow(3 * pi * pi * rt + 1e-20, third);
+  const D4 ks = dsqrt(4 * kf / pi);
+  const D4 gn = dsqrt(gx * gx + gy * gy + gz * gz + 1e-30);
+  const D4 t = gn / dclip(2 * ks * rt, 1e-20);
+  const D4 dA = gamma * dexpm1(-1.0 * eps_pw / gamma);
+  const D4 Ac = beta / dclip(dA, 1e-20);
+  const D4 t2 = t * t;
+  const D4 f1 = t2 + Ac * (t2 * t2);
+  const D4 frac = beta * f1 / dclip(gamma * (1.0 + Ac * f1), 1e-20);
+  const D4 H = gamma * dlog1p(frac);
+  return xs * ex + cs * (eps_pw + H);
+}
+
+// per point: rho, grad in, v_rho, v_grad out (in place); e per block
+__global__ void __launch_bounds__(kPtThreads) pbe_kernel(double* __restrict__ rho,
+                                                         double* __restrict__ grad,
+                                                         const double* __restrict__ w, int64_t G,
+                                                         int64_t ng, double xs, double cs,
+                                                         double thresh, double* __restrict__ ered) {
+  __shared__ double red[kPtThreads];
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (g < ng) {
+    const double r = rho[g];
+    double vr = 0.0, v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    if (r > thresh) {
+      const double wg = w[g];
+      const D4 R = {r, {1.0, 0.0, 0.0, 0.0}};
+      const D4 X = {grad[g], {0.0, 1.0, 0.0, 0.0}};
+      const D4 Y = {grad[G + g], {0.0, 0.0, 1.0, 0.0}};
+      const D4 Z = {grad[2 * G + g], {0.0, 0.0, 0.0, 1.0}};
+      const D4 f = R * pbe_eps(R, X, Y, Z, xs, cs);
+      e = wg * f.v;
+      vr = wg * f.d[0];
+      v0 = wg * f.d[1];
+      v1 = wg * f.d[2];
+      v2 = wg * f.d[3];
+    }
+    rho[g] = vr;
+    grad[g] = v0;
+    grad[G + g] = v1;
+    grad[2 * G + g] = v2;
+  }
+  red[threadIdx.x] = e;
+  __syncthreads();
+  for (int o = kPtThreads / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) ered[blockIdx.x] = red[0];
+}
+
+// W[mu][g] = v_rho/2 Phi + v_grad . dPhi (zero past ng)
+__global__ void w_kernel(const double* __restrict__ phi, const double* __restrict__ dphi,
+                         const double* __restrict__ vr, const double* __restrict__ vg, int nao,
+                         int64_t G, int64_t ng, double* __restrict__ W) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t plane = (int64_t)nao * G;
+  if (i >= plane) return;
+  const int64_t g = i % G;
+  double v = 0.0;
+  if (g < ng)
+    v = 0.5 * vr[g] * phi[i] + vg[g] * dphi[i] + vg[G + g] * dphi[plane + i] +
+        vg[2 * G + g] * dphi[2 * plane + i];
+  W[i] = v;
+}
+
+__global__ void symmetrize_add_kernel(const double* __restrict__ V, int n, double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n * n) return;
+  const int64_t r = i / n, c = i % n;
+  out[i] = V[i] + V[c * n + r];
+}
+
+}  // namespace
+
+void launch_becke_partition(const double* pts, const int* owner, const double* raw, int64_t n,
+                            const double* atom_xyz, const double* bragg, int natom, double* w,
+                            cudaStream_t s) {
+  if (n <= 0) return;
+  // pair tables: 1 / R_AB and the size adjustment a_AB (becke.py: becke_partition)
+  std::vector<double> inv((size_t)natom * natom, 0.0), aab((size_t)natom * natom, 0.0);
+  for (int a = 0; a < natom; ++a)
+    for (int b = 0; b < natom; ++b) {
+      if (a == b) continue;
+      const double dx = atom_xyz[3 * a] - atom_xyz[3 * b], dy = atom_xyz[3 * a + 1] - atom_xyz[3 * b + 1],
+                   dz = atom_xyz[3 * a + 2] - atom_xyz[3 * b + 2];
+      inv[(size_t)a * natom + b] = 1.0 / std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double chi = bragg[a] / bragg[b];
+      const double u = (chi - 1.0) / (chi + 1.0);
+      aab[(size_t)a * natom + b] = std::min(0.45, std::max(-0.45, u / (u * u - 1.0)));
+    }
+  std::vector<double> xyz(atom_xyz, atom_xyz + 3 * natom);
+  DevBuf dxyz, dinv, daab;
+  upload(dxyz, xyz);
+  upload(dinv, inv);
+  upload(daab, aab);
+  int threads = 64;
+  const size_t smem = (size_t)natom * threads * sizeof(double);
+  if (smem > 200 * 1024) fail(DFJK_ERR_UNSUPPORTED, "Becke partition supports at most 400 atoms");
+  DFJK_CUDA(cudaFuncSetAttribute(becke_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)std::max<size_t>(smem, 1)));
+  becke_kernel<<<(unsigned)((n + threads - 1) / threads), threads, smem, s>>>(
+      pts, owner, raw, n, dxyz.as<double>(), dinv.as<double>(), daab.as<double>(), natom, w);
+  DFJK_LAUNCHED();
+  DFJK_CUDA(cudaStreamSynchronize(s));   // the pair tables are freed on return
+}
+
+double xc_energy_fock(const Context& c, const OrbView& ov, int nshell, const double* pts,
+                      const double* w, int64_t npts, const double* P, double* Vxc,
+                      const XcParams& xp, XcWork& ws, cudaStream_t s) {
+  const int nao = ov.nao;
+  int64_t G = ws.chunk;
+  if (G <= 0) {
+    // about 1.5 GB of chunk buffers: Phi, 3 dPhi, X, W
+    G = ((int64_t)1536 << 20) / (6 * 8 * (int64_t)nao);
+    G = std::max<int64_t>(1024, std::min<int64_t>(G, 65536)) / kPtThreads * kPtThreads;
+    ws.chunk = G;
+  }
+  const int64_t plane = (int64_t)nao * G;
+  ws.phi.ensure(plane * sizeof(double));
+  ws.dphi.ensure(3 * plane * sizeof(double));
+  ws.X.ensure(plane * sizeof(double));
+  ws.W.ensure(plane * sizeof(double));
+  ws.vr.ensure(G * sizeof(double));
+  ws.vg.ensure(3 * G * sizeof(double));
+  const int64_t nchunk = (npts + G - 1) / G;
+  const int64_t nblk = G / kPtThreads;
+  ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
+  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+  DevBuf vacc;
+  if (Vxc) {
+    vacc.alloc((size_t)nao * nao * sizeof(double));
+    DFJK_CUDA(cudaMemsetAsync(vacc.p, 0, (size_t)nao * nao * sizeof(double), s));
+  }
+  const double one = 1.0, zero = 0.0;
+  for (int64_t ch = 0; ch < nchunk; ++ch) {
+    const int64_t g0 = ch * G, ng = std::min(G, npts - g0);
+    ao_kernel<<<dim3((unsigned)((G + kAoThreads - 1) / kAoThreads), (unsigned)nshell), kAoThreads, 0,
+                s>>>(ov, pts, g0, ng, G, ws.phi.as<double>(), ws.dphi.as<double>());
+    DFJK_LAUNCHED();
+    // X (G x nao, column-major: [mu][g]) = Phi P
+    DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nao, nao, &one,
+                            ws.phi.as<double>(), (int)G, P, nao, &zero, ws.X.as<double>(), (int)G));
+    rho_kernel<<<(unsigned)((ng + kPtThreads - 1) / kPtThreads), kPtThreads, 0, s>>>(
+        ws.X.as<double>(), ws.phi.as<double>(), ws.dphi.as<double>(), nao, G, ng,
+        ws.vr.as<double>(), ws.vg.as<double>());
+    DFJK_LAUNCHED();
+    pbe_kernel<<<(unsigned)nblk, kPtThreads, 0, s>>>(ws.vr.as<double>(), ws.vg.as<double>(),
+                                                     w + g0, G, ng, xp.x_scale, xp.c_scale,
+                                                     xp.rho_thresh,
+                                                     ws.ered.as<double>() + ch * nblk);
+    DFJK_LAUNCHED();
+    if (Vxc) {
+      w_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(
+          ws.phi.as<double>(), ws.dphi.as<double>(), ws.vr.as<double>(), ws.vg.as<double>(), nao, G,
+          ng, ws.W.as<double>());
+      DFJK_LAUNCHED();
+      // V += Phi^T W
+      DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, nao, nao, (int)G, &one,
+                              ws.phi.as<double>(), (int)G, ws.W.as<double>(), (int)G, &one,
+                              vacc.as<double>(), nao));
+    }
+  }
+  if (Vxc) {
+    const int64_t n2 = (int64_t)nao * nao;
+    symmetrize_add_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(vacc.as<double>(), nao, Vxc);
+    DFJK_LAUNCHED();
+  }
+  std::vector<double> e((size_t)nchunk * nblk);
+  if (!e.empty())
+    DFJK_CUDA(cudaMemcpyAsync(e.data(), ws.ered.p, e.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  double sum = 0.0;
+  for (double v : e) sum += v;
+  return sum;
+}
+
+}  // namespace dfjk

@@ -263,8 +263,9 @@ def eval_ao(basis, pts):
     return val, grad
 
 
-def pbe0_eps(torch, rho, grad):
-    """eps_xc of PBE0 per particle, as dftax's PBE0.__call__ (unpolarized)."""
+def pbe0_eps(torch, rho, grad, xs=0.75, cs=1.0):
+    """eps_xc per particle of xs PBE exchange + cs PBE correlation (PBE0 by
+    default, as dftax's PBE0.__call__; PBE with xs = 1), unpolarized."""
     pi = math.pi
     kappa, mu = 0.804, 0.2195149727645171
     gnorm = torch.linalg.norm(grad + 1e-30, dim=-1)
@@ -289,10 +290,10 @@ def pbe0_eps(torch, rho, grad):
     f1 = t ** 2 + Ac * t ** 4
     frac = beta * f1 / torch.clamp(gamma * (1.0 + Ac * f1), min=1e-20)
     H = gamma * torch.log1p(frac)
-    return 0.75 * ex + eps_pw + H
+    return xs * ex + cs * (eps_pw + H)
 
 
-def exc_and_vxc(basis, pts, w, P, ao=None):
+def exc_and_vxc(basis, pts, w, P, ao=None, xs=0.75, cs=1.0):
     """E_xc of PBE0 for the closed-shell density P and its P-gradient V_xc,
     symmetrized like dftax's Fock (scf.py:42-46)."""
     import torch
@@ -309,7 +310,7 @@ def exc_and_vxc(basis, pts, w, P, ao=None):
     mask = rho > 1e-10
     safe_rho = t.where(mask, rho, t.ones_like(rho))
     safe_grad = t.where(mask[:, None], grho, t.zeros_like(grho))
-    eps = pbe0_eps(t, safe_rho, safe_grad)
+    eps = pbe0_eps(t, safe_rho, safe_grad, xs, cs)
     wt = t.as_tensor(np.asarray(w, dtype=np.float64))
     e = t.sum(t.where(mask, wt * eps * rho, t.zeros_like(rho)))
     e.backward()
@@ -348,7 +349,8 @@ def _diis(dF, dE, count, m):
 class KSEnergy:
     """E(P) and F(P) of a closed-shell DF-PBE0 Kohn-Sham model (nspin = 1)."""
 
-    def __init__(self, orb, aux, coords, charges, pts, w, hf_coeff=0.25, I3=None, vinv=None):
+    def __init__(self, orb, aux, coords, charges, pts, w, hf_coeff=0.25, I3=None, vinv=None,
+                 xs=0.75, cs=1.0):
         self.S, T, V = one_electron(orb, coords, charges)
         self.hcore = T + V
         self.e_nn = nuclear_repulsion(coords, charges)
@@ -358,13 +360,17 @@ class KSEnergy:
         self.ao = eval_ao(orb, pts)
         self.orb = orb
         self.hf = hf_coeff
+        self.xs, self.cs = xs, cs
 
     def energy_fock(self, P):
         e1 = float(np.sum(P * self.hcore))
         e2 = odf.df_energy(self.I3, self.vinv, P[None], self.hf)
         J, _ = odf.df_jk(self.I3, self.vinv, P)
         K = odf.df_k(self.I3, self.vinv, P)
-        exc, vxc = exc_and_vxc(self.orb, self.pts, self.w, P, self.ao)
+        if self.xs == 0.0 and self.cs == 0.0:
+            exc, vxc = 0.0, np.zeros_like(P)
+        else:
+            exc, vxc = exc_and_vxc(self.orb, self.pts, self.w, P, self.ao, self.xs, self.cs)
         F = self.hcore + J - 0.5 * self.hf * K + vxc
         return e1 + e2 + exc + self.e_nn, 0.5 * (F + F.T)
 

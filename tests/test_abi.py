@@ -1,5 +1,5 @@
 """C ABI and host logic, no GPU needed: the library loads and exports every
-entry point include/dfjk.h declares; the synthetic workloads are what the
+entry point include/dfjk.h and include/dfscf.h declare; the synthetic workloads are what the
 configs describe."""
 
 import ctypes
@@ -14,9 +14,12 @@ from dftax_b200 import _lib, systems
 
 
 def header_functions():
-    src = open(os.path.join(ROOT, "include", "dfjk.h")).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return set(re.findall(r"\b(dfjk_[a-z0-9_]+)\s*\(", src))
+    names = set()
+    for h in ("dfjk.h", "dfscf.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"\b((?:dfjk|dfscf)_[a-z0-9_]+)\s*\(", src))
+    return names
 
 
 def test_exports_match_header():
