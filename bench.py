@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scf-steps", type=int, default=2,
+                    help="timed SCF solves per precision (0: no SCF measurement)")
     ap.add_argument("--screen", type=float, default=0.0,
                     help="relative Schwarz screen of shell pairs (0: none, the default)")
     return ap.parse_args()
@@ -455,6 +457,8 @@ def run_ours(args, rank, world, local_rank):
             "rel_dJ": float(np.linalg.norm(r["J"] - f["J"]) / np.linalg.norm(f["J"])),
             "rel_dK": float(np.linalg.norm(r["K"] - f["K"]) / np.linalg.norm(f["K"])),
             "energy": "DFCoulomb energy of P = 2 C C^T with a_x = 0.25 (PBE0 exchange share)"}
+    if args.scf_steps > 0:
+        line["scf"] = scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         secs, parts, n = cpu_full_builds(args.workload, 1)
         line["cpu_baseline"] = {"value": round(1.0 / secs[0], 6), "unit": UNIT, "cores": n,
@@ -468,6 +472,52 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks):
+    """SCF solves/s of the workload from geometry, per precision: the DF plan
+    and build, the Becke grid (75 radial shells, 302-point Lebedev, NWChem
+    pruning), one-electron integrals and the DIIS iterations of a closed-shell
+    DF-PBE0 SCF from the core-Hamiltonian guess, to |dE| < 1e-8 Ha and a
+    commutator below 1e-6 (dftax's defaults). One untimed solve first."""
+    from dftax_b200 import df
+    from dftax_b200.ks import KS, scf
+
+    out = {}
+    res = {}
+    for prec in precs:
+        def solve():
+            ks = KS(sym, xyz, orb, coulomb=df(aux, precision=prec))
+            r = scf(ks)
+            ks.close()
+            ks.plan.close()
+            return r
+
+        solve()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rs = [solve() for _ in range(args.scf_steps)]
+        torch.cuda.synchronize()
+        sec = max_over_ranks(time.perf_counter() - t0)
+        r = rs[-1]
+        res[prec] = r
+        it_ms = sum(r.timings_ms.values())
+        out[prec] = {"value": round(world * args.scf_steps / sec, 4), "unit": "SCF solves/s",
+                     "ms_per_solve": round(1e3 * sec / args.scf_steps, 2),
+                     "n_iter": r.n_iter, "converged": r.converged, "e_tot_Ha": r.e_tot,
+                     "iteration_parts_ms": {k: round(v, 2) for k, v in r.timings_ms.items()},
+                     "setup_ms": round(1e3 * sec / args.scf_steps - it_ms, 2)}
+    head = precs[0]
+    line = dict(out[head])
+    line["precision"] = head
+    line["what"] = ("one closed-shell DF-PBE0 SCF from geometry: plan and DF build, Becke grid "
+                    "(75 x 302, NWChem pruning), one-electron integrals, core guess, DIIS to "
+                    "|dE| < 1e-8 Ha and commutator < 1e-6")
+    if "fp64" in out and head != "fp64":
+        line["fp64"] = out["fp64"]
+        line["speedup_vs_fp64"] = round(out["fp64"]["ms_per_solve"] / out[head]["ms_per_solve"], 3)
+        line["abs_dE_vs_fp64_Ha"] = abs(res[head].e_tot - res["fp64"].e_tot)
+    return line
 
 
 def workload_config(args, orb, aux, nocc, world):

@@ -77,7 +77,8 @@ class ScfResult(ctypes.Structure):
     _fields_ = [("e_tot", c_double), ("e_one", c_double), ("e_coul", c_double),
                 ("e_xc", c_double), ("e_nn", c_double), ("derr", c_double),
                 ("n_iter", c_int32), ("converged", c_int32), ("nmo", c_int32),
-                ("nocc", c_int32)]
+                ("nocc", c_int32), ("ms_jk", c_double), ("ms_xc", c_double),
+                ("ms_diag", c_double), ("ms_diis", c_double)]
 
 
 _lib = None

@@ -25,6 +25,7 @@
 #include "scf.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 
 namespace dfjk {
@@ -92,6 +93,23 @@ __global__ void antisym_kernel(const double* __restrict__ Bm, int n, double* __r
 
 unsigned blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
+// adds the milliseconds of the device work enqueued on s since the last mark
+struct PartTimer {
+  cudaStream_t s;
+  std::chrono::steady_clock::time_point t0;
+  explicit PartTimer(cudaStream_t st) : s(st) { mark(); }
+  void mark() {
+    DFJK_CUDA(cudaStreamSynchronize(s));
+    t0 = std::chrono::steady_clock::now();
+  }
+  void add(double& acc) {
+    DFJK_CUDA(cudaStreamSynchronize(s));
+    const auto t1 = std::chrono::steady_clock::now();
+    acc += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    t0 = t1;
+  }
+};
+
 double ddot(Context& c, const double* a, const double* b, int64_t n, cudaStream_t s) {
   double r = 0.0;
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
@@ -140,6 +158,7 @@ double energy_fock(dfscf& f, const double* P, bool from_orbitals, double* Fout, 
   const int64_t n = f.nao, nn = n * n;
   const double hf = f.o.hf_coeff;
   double e_coul;
+  PartTimer tm(s);
   if (from_orbitals) {
     // C_occ row-major [nao][nocc] for the plan's J/K; weight 2 per orbital
     const double one = 1.0, zero = 0.0;
@@ -161,12 +180,14 @@ double energy_fock(dfscf& f, const double* P, bool from_orbitals, double* Fout, 
                                            0.0, nn, Fout);
     DFJK_LAUNCHED();
   }
+  tm.add(f.res.ms_jk);
   double e_xc = 0.0;
   if (has_xc(f)) {
     e_xc = xc_energy_fock(c, f.ov, f.nshell, f.pts.as<double>(), f.wts.as<double>(), f.npts, P,
                           f.Vxc.as<double>(), xc_params(f), f.xcw, s);
     add_inplace_kernel<<<blocks(nn), 256, 0, s>>>(f.Vxc.as<double>(), nn, Fout);
     DFJK_LAUNCHED();
+    tm.add(f.res.ms_xc);
   }
   const double e_one = ddot(c, P, f.H.as<double>(), nn, s);
   f.res.e_one = e_one;
@@ -179,6 +200,7 @@ double energy_fock(dfscf& f, const double* P, bool from_orbitals, double* Fout, 
 // orbitals of F into f.C / f.eps and the aufbau density into f.P
 void make_density(dfscf& f, const double* Fm, cudaStream_t s) {
   Context& c = *f.c;
+  PartTimer tm(s);
   const int n = f.nao, m = f.nmo;
   // Fo = X^T F X
   gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, m, n, 1.0, Fm, n, f.X.as<double>(), n, 0.0, f.A1.as<double>(),
@@ -196,6 +218,7 @@ void make_density(dfscf& f, const double* Fm, cudaStream_t s) {
                           f.C.as<double>(), n, &zero, f.P.as<double>(), n));
   fill_upper_kernel<<<blocks((int64_t)n * n), 256, 0, s>>>(f.P.as<double>(), n);
   DFJK_LAUNCHED();
+  tm.add(f.res.ms_diag);
   f.have_orbitals = true;
 }
 
@@ -283,6 +306,7 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
   bool converged = false;
   double derr = INFINITY;
   while (it < f.o.max_iter && !converged) {
+    PartTimer tm(s);
     const int slot = it % md;
     double* dFs = f.dF.as<double>() + slot * nn;
     double* dEs = f.dE.as<double>() + slot * mm;
@@ -319,6 +343,7 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
     }
     // the DIIS Fock moves to the dedicated buffer before make_density reuses A1/A2
     DFJK_CUDA(cudaMemcpyAsync(f.Vxc.p, Fext, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    tm.add(f.res.ms_diis);
     make_density(f, f.Vxc.as<double>(), s);
     const double e = energy_fock(f, f.P.as<double>(), true, f.F.as<double>(), s);
     converged = std::fabs(e - e_prev) < f.o.e_tol && derr < f.o.d_tol;

@@ -48,6 +48,7 @@ class KSResult:
     P: np.ndarray             # (1, nao, nao)
     e_xc: float = 0.0
     e_coul: float = 0.0
+    timings_ms: dict | None = None   # J/K, XC, diagonalization, DIIS of the run
 
 
 class KS:
@@ -193,7 +194,9 @@ def scf(ks: KS, *, max_iter: int = 128, e_tol: float = 1e-8, d_tol: float = 1e-6
     return KSResult(e_tot=r.e_tot, e_elec=r.e_tot - r.e_nn, converged=bool(r.converged),
                     n_iter=r.n_iter, nocc=ks.nocc, mo_energy=eps.cpu().numpy()[None],
                     mo_coeff=C.T.cpu().numpy()[None], P=P.cpu().numpy()[None], e_xc=r.e_xc,
-                    e_coul=r.e_coul)
+                    e_coul=r.e_coul,
+                    timings_ms={"jk": r.ms_jk, "xc": r.ms_xc, "diag": r.ms_diag,
+                                "diis": r.ms_diis})
 
 
 __all__ = ["KS", "KSResult", "scf", "XC_FUNCTIONALS"]

@@ -52,6 +52,10 @@ typedef struct {
   int32_t converged;
   int32_t nmo;          /* orbitals kept by the canonical orthonormalizer               */
   int32_t nocc;
+  /* milliseconds of the last dfscf_run by part (host clock around
+   * synchronized device work): J and K, the XC quadrature, the Fock
+   * diagonalizations with the density, the commutator and DIIS */
+  double ms_jk, ms_xc, ms_diag, ms_diis;
 } dfscf_result;
 
 /* dftax's defaults for PBE0 (scf.py:279-391, xc.py:584-601, grid.py:10-45). */
