@@ -69,7 +69,8 @@ class PlanInfo(ctypes.Structure):
 class ScfOptions(ctypes.Structure):
     _fields_ = [("hf_coeff", c_double), ("x_scale", c_double), ("c_scale", c_double),
                 ("e_tol", c_double), ("d_tol", c_double), ("lindep", c_double),
-                ("level_shift", c_double), ("rho_thresh", c_double), ("max_iter", c_int32),
+                ("level_shift", c_double), ("rho_thresh", c_double), ("ao_thresh", c_double),
+                ("max_iter", c_int32),
                 ("diis_space", c_int32), ("grid_chunk", c_int64)]
 
 

@@ -183,8 +183,8 @@ double energy_fock(dfscf& f, const double* P, bool from_orbitals, double* Fout, 
   tm.add(f.res.ms_jk);
   double e_xc = 0.0;
   if (has_xc(f)) {
-    e_xc = xc_energy_fock(c, f.ov, f.nshell, f.pts.as<double>(), f.wts.as<double>(), f.npts, P,
-                          f.Vxc.as<double>(), xc_params(f), f.xcw, s);
+    e_xc = xc_energy_fock(c, f.ov, f.pts.as<double>(), f.wts.as<double>(), P, f.Vxc.as<double>(),
+                          xc_params(f), f.xcw, s);
     add_inplace_kernel<<<blocks(nn), 256, 0, s>>>(f.Vxc.as<double>(), nn, Fout);
     DFJK_LAUNCHED();
     tm.add(f.res.ms_xc);
@@ -374,6 +374,7 @@ void dfscf_default_options(dfscf_options* o) {
   o->lindep = 1e-7;
   o->level_shift = 0.0;
   o->rho_thresh = 1e-10;
+  o->ao_thresh = 1e-14;
   o->max_iter = 128;
   o->diis_space = 8;
   o->grid_chunk = 0;
@@ -410,12 +411,19 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     f->natom = natom;
     f->npts = npoint;
     f->nshell = p.orb.n;
-    f->xcw.chunk = f->o.grid_chunk > 0 ? (f->o.grid_chunk + 255) / 256 * 256 : 0;
+
     upload(f->atom_xyz, std::vector<double>(atom_xyz, atom_xyz + 3 * natom));
     upload(f->atom_z, std::vector<double>(atom_charge, atom_charge + natom));
+    if (!(f->o.ao_thresh >= 0.0)) fail(DFJK_ERR_INVALID, "ao_thresh must be >= 0");
     if (npoint > 0) {
-      upload(f->pts, std::vector<double>(grid_xyz, grid_xyz + 3 * npoint));
-      upload(f->wts, std::vector<double>(grid_w, grid_w + npoint));
+      // spatially sorted chunks with their non-negligible shells
+      std::vector<double> pv(grid_xyz, grid_xyz + 3 * npoint), wv(grid_w, grid_w + npoint);
+      const int64_t G = f->o.grid_chunk > 0 ? (f->o.grid_chunk + 255) / 256 * 256 : 8192;
+      int nout[8];
+      for (int l = 0; l < 8; ++l) nout[l] = p.orb.spherical ? 2 * l + 1 : ncart(l);
+      xc_prepare(p.orb, nout, pv, wv, G, f->o.ao_thresh, f->xcw.ch);
+      upload(f->pts, pv);
+      upload(f->wts, wv);
     }
     double enn = 0.0;
     for (int a = 0; a < natom; ++a)
@@ -551,8 +559,15 @@ dfjk_status dfscf_xc(dfscf* f, const double* P, double* exc, double* Vxc, void* 
   if (!f || !P || !exc) return DFJK_ERR_INVALID;
   return guard(f->c, [&] {
     DFJK_CUDA(cudaSetDevice(f->c->device));
-    *exc = xc_energy_fock(*f->c, f->ov, f->nshell, f->pts.as<double>(), f->wts.as<double>(), f->npts,
-                          P, Vxc, xc_params(*f), f->xcw, static_cast<cudaStream_t>(stream));
+    if (!has_xc(*f)) {
+      *exc = 0.0;
+      if (Vxc)
+        DFJK_CUDA(cudaMemsetAsync(Vxc, 0, (size_t)f->nao * f->nao * sizeof(double),
+                                  static_cast<cudaStream_t>(stream)));
+      return;
+    }
+    *exc = xc_energy_fock(*f->c, f->ov, f->pts.as<double>(), f->wts.as<double>(), P, Vxc,
+                          xc_params(*f), f->xcw, static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -24,12 +24,33 @@ void launch_one_electron(const Context& c, const OrbView& ov, int nshell, const 
                          int natom, const double* atom_xyz, const double* atom_z, double* S,
                          double* T, double* V, cudaStream_t s);
 
+// Chunks of spatially sorted grid points, each with the orbital shells that
+// are not negligible anywhere in its bounding box (xc_prepare)
+struct XcChunks {
+  int64_t G = 0;                       // points per chunk (the last may hold fewer)
+  std::vector<int64_t> g0, ng;         // first point and count of each chunk
+  std::vector<int> sh_off, sh_cnt;     // each chunk's range in the shell list
+  std::vector<int64_t> ao_off;         // each chunk's range in the compact AO map
+  std::vector<int> ao_cnt;
+  int max_ao = 0;
+  int64_t total_ao = 0;                // sum of ao_cnt (the dense form would be nchunk * nao)
+  DevBuf d_sh, d_sh_out0, d_ao_map;    // shells, their first compact AO, compact -> AO
+};
+
 // XC on a point grid (xc.cu)
 struct XcWork {
-  int64_t chunk = 0;            // points per chunk
-  DevBuf phi, dphi, X, W;       // [nao][chunk] AO values, 3 gradients, Phi P, weighted AO
+  XcChunks ch;
+  DevBuf phi, dphi, X, W;       // [nsig][G] AO values, 3 gradients, Phi P, weighted AO
+  DevBuf Pc, Vc, Vacc;          // P on a chunk's AOs, its V block, V accumulated
   DevBuf vr, vg, ered;          // per point: v_rho, v_grad (3), energy partials per block
 };
+
+// Sorts the points (and weights) along a Morton curve over 1-Bohr cells, cuts
+// them into chunks of G points and keeps for each chunk the shells whose
+// value-and-gradient bound over the chunk's bounding box exceeds thresh.
+// pts [n][3] and w [n] are host arrays, reordered in place.
+void xc_prepare(const Shells& sh, const int (&nout)[8], std::vector<double>& pts,
+                std::vector<double>& w, int64_t G, double thresh, XcChunks& out);
 
 struct XcParams {
   double x_scale = 0.75;        // PBE exchange share (PBE0)
@@ -39,11 +60,12 @@ struct XcParams {
 
 // E_xc of the closed-shell density P (nao x nao, symmetric, device) and, when
 // Vxc != nullptr, its P-gradient symmetrized (device, nao x nao), over the grid
-// points pts [n][3] with weights w [n] (device). Uses the context's cuBLAS
-// handle on stream s. Returns E_xc (host synchronizing).
-double xc_energy_fock(const Context& c, const OrbView& ov, int nshell, const double* pts,
-                      const double* w, int64_t npts, const double* P, double* Vxc,
-                      const XcParams& xp, XcWork& ws, cudaStream_t s);
+// points pts [n][3] with weights w [n] (device, in xc_prepare's order), chunk
+// by chunk as ws.ch lays them out. Uses the context's cuBLAS handle on
+// stream s. Returns E_xc (host synchronizing).
+double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, const double* w,
+                      const double* P, double* Vxc, const XcParams& xp, XcWork& ws,
+                      cudaStream_t s);
 
 // Becke cell weights: w[i] = raw[i] * P_owner(i) / sum_A P_A at point i
 void launch_becke_partition(const double* pts, const int* owner, const double* raw, int64_t n,

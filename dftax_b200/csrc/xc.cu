@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <utility>
 
 namespace dfjk {
 namespace {
@@ -75,18 +76,22 @@ __device__ __forceinline__ double ipow(double x, int n) {
   return r;
 }
 
-// Phi[mu][g] (ld G), dPhi[x][mu][g]; grid (ceil(ng / 128), nshell)
-__global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const double* __restrict__ pts,
-                                                        int64_t g0, int64_t ng, int64_t G,
+// Phi[k][g] (ld G), dPhi[x][k][g] for the chunk's shells: shell j of the
+// chunk is orbital shell sh[j] with compact AOs k = out0c[j] .. ; grid
+// (ceil(G / 128), shells of the chunk)
+__global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const int* __restrict__ shl,
+                                                        const int* __restrict__ out0c,
+                                                        const double* __restrict__ pts,
+                                                        int64_t g0, int64_t ng, int64_t G, int nsig,
                                                         double* __restrict__ phi,
                                                         double* __restrict__ dphi) {
   const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int s = blockIdx.y;
+  const int s = shl[blockIdx.y];
   if (g >= G) return;
   const ShellView& sh = ov.sh;
   const int l = sh.l[s], nc = (l + 1) * (l + 2) / 2, nout = ov.nout[l];
-  const int64_t mu0 = ov.out0[s];
-  const int64_t plane = (int64_t)ov.nao * G;
+  const int64_t mu0 = out0c[blockIdx.y];
+  const int64_t plane = (int64_t)nsig * G;
   double val[10] = {}, gx[10] = {}, gy[10] = {}, gz[10] = {};
   if (g < ng) {
     const double* p = pts + 3 * (g0 + g);
@@ -131,6 +136,24 @@ __global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const double
     dphi[plane + o] = b;
     dphi[2 * plane + o] = c;
   }
+}
+
+// Pc[k1][k2] = P[map[k1]][map[k2]]
+__global__ void gather_p_kernel(const double* __restrict__ P, int nao, const int* __restrict__ map,
+                                int nsig, double* __restrict__ Pc) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)nsig * nsig) return;
+  const int64_t a = i / nsig, b = i % nsig;
+  Pc[i] = P[(int64_t)map[a] * nao + map[b]];
+}
+
+// V[map[k1]][map[k2]] += Vc[k1][k2] (column-major Vc; the map is one-to-one)
+__global__ void scatter_v_kernel(const double* __restrict__ Vc, int nsig, const int* __restrict__ map,
+                                 int nao, double* __restrict__ V) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)nsig * nsig) return;
+  const int64_t a = i % nsig, b = i / nsig;
+  V[(int64_t)map[b] * nao + map[a]] += Vc[i];
 }
 
 // rho[g] = sum_mu X Phi, grad[x][g] = 2 sum_mu X dPhi_x
@@ -352,65 +375,175 @@ void launch_becke_partition(const double* pts, const int* owner, const double* r
   DFJK_CUDA(cudaStreamSynchronize(s));   // the pair tables are freed on return
 }
 
-double xc_energy_fock(const Context& c, const OrbView& ov, int nshell, const double* pts,
-                      const double* w, int64_t npts, const double* P, double* Vxc,
-                      const XcParams& xp, XcWork& ws, cudaStream_t s) {
-  const int nao = ov.nao;
-  int64_t G = ws.chunk;
-  if (G <= 0) {
-    // about 1.5 GB of chunk buffers: Phi, 3 dPhi, X, W
-    G = ((int64_t)1536 << 20) / (6 * 8 * (int64_t)nao);
-    G = std::max<int64_t>(1024, std::min<int64_t>(G, 65536)) / kPtThreads * kPtThreads;
-    ws.chunk = G;
+// interleaves the low 21 bits of x, y, z (Morton order)
+static uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
+  auto spread = [](uint64_t v) {
+    v &= 0x1fffffULL;
+    v = (v | v << 32) & 0x1f00000000ffffULL;
+    v = (v | v << 16) & 0x1f0000ff0000ffULL;
+    v = (v | v << 8) & 0x100f00f00f00f00fULL;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+    v = (v | v << 2) & 0x1249249249249249ULL;
+    return v;
+  };
+  return spread(x) | spread(y) << 1 | spread(z) << 2;
+}
+
+void xc_prepare(const Shells& sh, const int (&nout)[8], std::vector<double>& pts,
+                std::vector<double>& w, int64_t G, double thresh, XcChunks& out) {
+  const int64_t n = (int64_t)w.size();
+  out.g0.clear();
+  out.ng.clear();
+  out.sh_off.clear();
+  out.sh_cnt.clear();
+  out.ao_off.clear();
+  out.ao_cnt.clear();
+  out.max_ao = 0;
+  out.total_ao = 0;
+  out.G = G;
+  if (n == 0) return;
+  // Morton order of 1-Bohr cells
+  double lo[3] = {INFINITY, INFINITY, INFINITY};
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], pts[3 * i + d]);
+  std::vector<std::pair<uint64_t, int64_t>> key(n);
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t c[3];
+    for (int d = 0; d < 3; ++d) c[d] = (uint64_t)std::floor(pts[3 * i + d] - lo[d]);
+    key[i] = {morton3(c[0], c[1], c[2]), i};
   }
-  const int64_t plane = (int64_t)nao * G;
-  ws.phi.ensure(plane * sizeof(double));
-  ws.dphi.ensure(3 * plane * sizeof(double));
-  ws.X.ensure(plane * sizeof(double));
-  ws.W.ensure(plane * sizeof(double));
+  std::sort(key.begin(), key.end());
+  std::vector<double> p2(3 * n), w2(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t j = key[i].second;
+    for (int d = 0; d < 3; ++d) p2[3 * i + d] = pts[3 * j + d];
+    w2[i] = w[j];
+  }
+  pts.swap(p2);
+  w.swap(w2);
+  // per shell: |phi| + |grad phi| <= sum_k |c_k| (1 + r^l + l r^(l-1) + 2 a_k r^(l+1)) e^(-a_k r^2)
+  // for r beyond the distance d from the shell to a box, each term taken at
+  // max(d, its peak) (the factors decrease past sqrt((l+1)/(2 a_k)))
+  auto bound = [&](int s, double d) {
+    const int l = sh.l[s];
+    double b = 0.0;
+    for (int k = 0; k < sh.nprim[s]; ++k) {
+      const double a = sh.pexp[sh.prim0[s] + k], c = std::fabs(sh.pcoef[sh.prim0[s] + k]);
+      const double r = std::max(d, std::sqrt((l + 1) / (2.0 * a)));
+      const double rl = std::pow(r, l);
+      b += c * (1.0 + rl + (l > 0 ? l * rl / r : 0.0) + 2.0 * a * rl * r) *
+           std::exp(-a * std::max(d, 0.0) * std::max(d, 0.0));
+    }
+    return b;
+  };
+  std::vector<int> shl, out0c, aomap;
+  for (int64_t g0 = 0; g0 < n; g0 += G) {
+    const int64_t ng = std::min(G, n - g0);
+    double bl[3] = {INFINITY, INFINITY, INFINITY}, bh[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = g0; i < g0 + ng; ++i)
+      for (int d = 0; d < 3; ++d) {
+        bl[d] = std::min(bl[d], pts[3 * i + d]);
+        bh[d] = std::max(bh[d], pts[3 * i + d]);
+      }
+    out.g0.push_back(g0);
+    out.ng.push_back(ng);
+    out.sh_off.push_back((int)shl.size());
+    out.ao_off.push_back((int64_t)aomap.size());
+    int nao_c = 0;
+    for (int s = 0; s < sh.n; ++s) {
+      double d2 = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        const double c = sh.cen[3 * s + d];
+        const double e = c < bl[d] ? bl[d] - c : (c > bh[d] ? c - bh[d] : 0.0);
+        d2 += e * e;
+      }
+      if (bound(s, std::sqrt(d2)) <= thresh) continue;
+      shl.push_back(s);
+      out0c.push_back(nao_c);
+      const int no = nout[sh.l[s]];
+      for (int m = 0; m < no; ++m) aomap.push_back(sh.out0[s] + m);
+      nao_c += no;
+    }
+    out.sh_cnt.push_back((int)shl.size() - out.sh_off.back());
+    out.ao_cnt.push_back(nao_c);
+    out.max_ao = std::max(out.max_ao, nao_c);
+    out.total_ao += nao_c;
+  }
+  upload(out.d_sh, shl);
+  upload(out.d_sh_out0, out0c);
+  upload(out.d_ao_map, aomap);
+}
+
+double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, const double* w,
+                      const double* P, double* Vxc, const XcParams& xp, XcWork& ws,
+                      cudaStream_t s) {
+  const int nao = ov.nao;
+  const XcChunks& ch = ws.ch;
+  const int64_t G = ch.G;
+  const int64_t nchunk = (int64_t)ch.g0.size();
+  const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
+  const int64_t plane_max = (int64_t)std::max(ch.max_ao, 1) * G;
+  ws.phi.ensure(plane_max * sizeof(double));
+  ws.dphi.ensure(3 * plane_max * sizeof(double));
+  ws.X.ensure(plane_max * sizeof(double));
+  ws.W.ensure(plane_max * sizeof(double));
+  ws.Pc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
+  ws.Vc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
   ws.vr.ensure(G * sizeof(double));
   ws.vg.ensure(3 * G * sizeof(double));
-  const int64_t nchunk = (npts + G - 1) / G;
-  const int64_t nblk = G / kPtThreads;
   ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
-  DevBuf vacc;
   if (Vxc) {
-    vacc.alloc((size_t)nao * nao * sizeof(double));
-    DFJK_CUDA(cudaMemsetAsync(vacc.p, 0, (size_t)nao * nao * sizeof(double), s));
+    ws.Vacc.ensure((size_t)nao * nao * sizeof(double));
+    DFJK_CUDA(cudaMemsetAsync(ws.Vacc.p, 0, (size_t)nao * nao * sizeof(double), s));
   }
   const double one = 1.0, zero = 0.0;
-  for (int64_t ch = 0; ch < nchunk; ++ch) {
-    const int64_t g0 = ch * G, ng = std::min(G, npts - g0);
-    ao_kernel<<<dim3((unsigned)((G + kAoThreads - 1) / kAoThreads), (unsigned)nshell), kAoThreads, 0,
-                s>>>(ov, pts, g0, ng, G, ws.phi.as<double>(), ws.dphi.as<double>());
+  for (int64_t k = 0; k < nchunk; ++k) {
+    const int64_t g0 = ch.g0[k], ng = ch.ng[k];
+    const int nsig = ch.ao_cnt[k], nsh = ch.sh_cnt[k];
+    const int* map = ch.d_ao_map.as<int>() + ch.ao_off[k];
+    if (nsig == 0) {
+      DFJK_CUDA(cudaMemsetAsync(ws.ered.as<double>() + k * nblk, 0, nblk * sizeof(double), s));
+      continue;
+    }
+    const int64_t plane = (int64_t)nsig * G;
+    ao_kernel<<<dim3((unsigned)((G + kAoThreads - 1) / kAoThreads), (unsigned)nsh), kAoThreads, 0,
+                s>>>(ov, ch.d_sh.as<int>() + ch.sh_off[k], ch.d_sh_out0.as<int>() + ch.sh_off[k],
+                     pts, g0, ng, G, nsig, ws.phi.as<double>(), ws.dphi.as<double>());
     DFJK_LAUNCHED();
-    // X (G x nao, column-major: [mu][g]) = Phi P
-    DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nao, nao, &one,
-                            ws.phi.as<double>(), (int)G, P, nao, &zero, ws.X.as<double>(), (int)G));
+    gather_p_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, s>>>(
+        P, nao, map, nsig, ws.Pc.as<double>());
+    DFJK_LAUNCHED();
+    // X (G x nsig, column-major: [k][g]) = Phi Pc
+    DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nsig, nsig, &one,
+                            ws.phi.as<double>(), (int)G, ws.Pc.as<double>(), nsig, &zero,
+                            ws.X.as<double>(), (int)G));
     rho_kernel<<<(unsigned)((ng + kPtThreads - 1) / kPtThreads), kPtThreads, 0, s>>>(
-        ws.X.as<double>(), ws.phi.as<double>(), ws.dphi.as<double>(), nao, G, ng,
+        ws.X.as<double>(), ws.phi.as<double>(), ws.dphi.as<double>(), nsig, G, ng,
         ws.vr.as<double>(), ws.vg.as<double>());
     DFJK_LAUNCHED();
     pbe_kernel<<<(unsigned)nblk, kPtThreads, 0, s>>>(ws.vr.as<double>(), ws.vg.as<double>(),
                                                      w + g0, G, ng, xp.x_scale, xp.c_scale,
-                                                     xp.rho_thresh,
-                                                     ws.ered.as<double>() + ch * nblk);
+                                                     xp.rho_thresh, ws.ered.as<double>() + k * nblk);
     DFJK_LAUNCHED();
     if (Vxc) {
       w_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(
-          ws.phi.as<double>(), ws.dphi.as<double>(), ws.vr.as<double>(), ws.vg.as<double>(), nao, G,
-          ng, ws.W.as<double>());
+          ws.phi.as<double>(), ws.dphi.as<double>(), ws.vr.as<double>(), ws.vg.as<double>(), nsig,
+          G, ng, ws.W.as<double>());
       DFJK_LAUNCHED();
-      // V += Phi^T W
-      DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, nao, nao, (int)G, &one,
-                              ws.phi.as<double>(), (int)G, ws.W.as<double>(), (int)G, &one,
-                              vacc.as<double>(), nao));
+      // Vc = Phi^T W, scattered into V
+      DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, nsig, nsig, (int)G, &one,
+                              ws.phi.as<double>(), (int)G, ws.W.as<double>(), (int)G, &zero,
+                              ws.Vc.as<double>(), nsig));
+      scatter_v_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, s>>>(
+          ws.Vc.as<double>(), nsig, map, nao, ws.Vacc.as<double>());
+      DFJK_LAUNCHED();
     }
   }
   if (Vxc) {
     const int64_t n2 = (int64_t)nao * nao;
-    symmetrize_add_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(vacc.as<double>(), nao, Vxc);
+    symmetrize_add_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(ws.Vacc.as<double>(), nao,
+                                                                        Vxc);
     DFJK_LAUNCHED();
   }
   std::vector<double> e((size_t)nchunk * nblk);

@@ -36,9 +36,12 @@ typedef struct {
   double lindep;        /* overlap eigenvalue cutoff of the orthonormalizer (1e-7)      */
   double level_shift;   /* Saunders-Hillier virtual shift, Ha (0)                       */
   double rho_thresh;    /* grid points with rho <= this are left out (1e-10)            */
+  double ao_thresh;     /* a shell is left out of a chunk of grid points when its value
+                           and gradient stay below this over the chunk (1e-14; 0: keep
+                           every shell, the dense quadrature)                          */
   int32_t max_iter;     /* 128                                                          */
   int32_t diis_space;   /* DIIS history depth (8)                                        */
-  int64_t grid_chunk;   /* points per XC chunk (0: chosen from nao)                     */
+  int64_t grid_chunk;   /* grid points per XC chunk, spatially sorted (0: 8192)         */
 } dfscf_options;
 
 typedef struct {

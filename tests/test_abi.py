@@ -94,3 +94,19 @@ def test_alkane_geometry():
 def test_workload_sizes(name, nao, naux, nocc):
     _, _, orb, aux, no = systems.workload(name)
     assert (orb.nao, aux.nao, no) == (nao, naux, nocc)
+
+
+def test_scf_default_options():
+    lib = _lib.load()
+    o = _lib.ScfOptions()
+    lib.dfscf_default_options(ctypes.byref(o))
+    assert (o.hf_coeff, o.x_scale, o.c_scale) == (0.25, 0.75, 1.0)       # PBE0
+    assert (o.e_tol, o.d_tol, o.max_iter, o.diis_space) == (1e-8, 1e-6, 128, 8)
+    assert o.lindep == 1e-7 and o.rho_thresh == 1e-10 and o.ao_thresh == 1e-14
+
+
+def test_scf_null_arguments_are_rejected():
+    lib = _lib.load()
+    assert lib.dfscf_create(None, 0, None, None, 0, None, None, 0, None, None) == 1
+    assert lib.dfscf_run(None, None, None, None) == 1
+    assert lib.dfscf_destroy(None) == 0
