@@ -1,4 +1,5 @@
-"""ctypes bindings of the C ABI declared in ``include/dfjk.h`` and ``include/dfscf.h``.
+"""ctypes bindings of the C ABI declared in ``include/dfjk.h``, ``include/dfscf.h`` and
+``include/dfbatch.h``.
 
 The library ``libdfjk.so`` is built in-tree by ``dftax_b200.build``. There is
 no fallback: if the library is missing or fails to load, every entry point
@@ -31,6 +32,9 @@ EXPORTS = (
     "dfscf_default_options", "dfscf_create", "dfscf_destroy", "dfscf_run", "dfscf_get_result",
     "dfscf_get_density", "dfscf_get_orbitals", "dfscf_one_electron", "dfscf_xc",
     "dfscf_energy_fock", "dfjk_becke_partition",
+    # include/dfbatch.h
+    "dfbatch_default_options", "dfbatch_create", "dfbatch_destroy", "dfbatch_submit",
+    "dfbatch_wait", "dfbatch_poll", "dfbatch_estimate",
 )
 PHASES = ("metric", "pairs", "eri3c", "bgemm", "j", "khalf", "ksyrk", "kplanes")
 
@@ -82,6 +86,23 @@ class ScfResult(ctypes.Structure):
                 ("ms_diag", c_double), ("ms_diis", c_double)]
 
 
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("workers", c_int32), ("reserved", c_int32), ("hbm_budget", c_int64)]
+
+
+class BatchRequest(ctypes.Structure):
+    _fields_ = [("orb", POINTER(Basis)), ("aux", POINTER(Basis)), ("plan_opts", Options),
+                ("natom", c_int32), ("nocc", c_int32), ("atom_xyz", c_void_p),
+                ("atom_charge", c_void_p), ("npoint", c_int64), ("grid_xyz", c_void_p),
+                ("grid_w", c_void_p), ("scf_opts", ScfOptions), ("P_out", c_void_p)]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [("status", c_int32), ("worker", c_int32), ("scf", ScfResult),
+                ("t_submit", c_double), ("t_start", c_double), ("t_end", c_double),
+                ("bytes", c_int64), ("message", ctypes.c_char * 256)]
+
+
 _lib = None
 
 
@@ -123,7 +144,7 @@ def load(path: str | None = None):
         "dfjk_energy_rsh": (c_int, [V, V, c_int32, c_double, c_double, P(c_double), V, V]),
         "dfscf_default_options": (None, [P(ScfOptions)]),
         "dfscf_create": (c_int, [V, c_int32, V, V, c_int64, V, V, c_int32, P(ScfOptions),
-                                 P(c_void_p)]),
+                                 P(c_void_p), V]),
         "dfscf_destroy": (c_int, [V]),
         "dfscf_run": (c_int, [V, V, P(ScfOptions), V]),
         "dfscf_get_result": (c_int, [V, P(ScfResult)]),
@@ -133,6 +154,13 @@ def load(path: str | None = None):
         "dfscf_xc": (c_int, [V, V, P(c_double), V, V]),
         "dfscf_energy_fock": (c_int, [V, V, P(c_double), V, V]),
         "dfjk_becke_partition": (c_int, [V, V, V, V, c_int64, c_int32, V, V, V, V]),
+        "dfbatch_default_options": (None, [P(BatchOptions)]),
+        "dfbatch_create": (c_int, [c_int, P(BatchOptions), P(c_void_p)]),
+        "dfbatch_destroy": (c_int, [V]),
+        "dfbatch_submit": (c_int, [V, P(BatchRequest), P(c_int64)]),
+        "dfbatch_wait": (c_int, [V, c_int64, P(BatchResult)]),
+        "dfbatch_poll": (c_int, [V, c_int64, P(c_int32)]),
+        "dfbatch_estimate": (c_int, [P(BatchRequest), P(c_int64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -149,6 +177,7 @@ def check(status: int, ctx=None):
         raise DfjkError(status, msg)
 
 
-__all__ = ["load", "check", "Basis", "Options", "PlanInfo", "ScfOptions", "ScfResult", "DfjkError",
+__all__ = ["load", "check", "Basis", "Options", "PlanInfo", "ScfOptions", "ScfResult",
+           "BatchOptions", "BatchRequest", "BatchResult", "DfjkError",
            "LibraryNotLoaded",
            "EXPORTS", "DFJK_FP64", "DFJK_MIXED", "byref"]

@@ -383,7 +383,7 @@ void dfscf_default_options(dfscf_options* o) {
 dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
                          const double* atom_charge, int64_t npoint, const double* grid_xyz,
                          const double* grid_w, int32_t nocc, const dfscf_options* opts,
-                         dfscf** out) {
+                         dfscf** out, void* stream) {
   if (!pl || !out) return DFJK_ERR_INVALID;
   *out = nullptr;
   dfscf* f = new (std::nothrow) dfscf;
@@ -448,7 +448,7 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     const int64_t n = p.nao, nn = n * n;
     for (DevBuf* b : {&f->S, &f->T, &f->V, &f->H, &f->P, &f->F, &f->J, &f->K, &f->Vxc, &f->A1, &f->A2})
       b->alloc(nn * sizeof(double));
-    cudaStream_t s = nullptr;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     launch_one_electron(*c, ov, f->nshell, p.orb.l, natom, f->atom_xyz.as<double>(),
                         f->atom_z.as<double>(), f->S.as<double>(), f->T.as<double>(),
                         f->V.as<double>(), s);
@@ -464,7 +464,8 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     w.alloc(n * sizeof(double));
     syevd(*f, f->A1.as<double>(), (int)n, w.as<double>(), s);
     std::vector<double> hw(n);
-    DFJK_CUDA(cudaMemcpy(hw.data(), w.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    DFJK_CUDA(cudaMemcpyAsync(hw.data(), w.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DFJK_CUDA(cudaStreamSynchronize(s));
     int first = 0;
     while (first < n && !(hw[first] > f->o.lindep)) ++first;
     f->nmo = (int)(n - first);
@@ -495,7 +496,9 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
 dfjk_status dfscf_destroy(dfscf* f) {
   if (!f) return DFJK_OK;
   cudaSetDevice(f->c->device);
-  cudaDeviceSynchronize();
+  // no device synchronization: the buffers go back to the library's cache,
+  // which synchronizes before it hands one out again unless the device has
+  // been synchronized since (solves on other streams keep running)
   delete f;
   return DFJK_OK;
 }

@@ -110,7 +110,7 @@ class KS:
                                          self.charges.ctypes.data, len(self.grid_weights),
                                          self.grid_coords.ctypes.data,
                                          self.grid_weights.ctypes.data, self.nocc[0], byref(o),
-                                         byref(self.h)), self.ctx.h)
+                                         byref(self.h), _stream_ptr(self.torch)), self.ctx.h)
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

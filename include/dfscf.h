@@ -67,12 +67,13 @@ void dfscf_default_options(dfscf_options* opts);
 /* An SCF over a built dfjk plan (closed shell, nocc doubly occupied orbitals).
  * atoms: natom centers (Bohr) and nuclear charges; grid: npoint points [n][3]
  * (Bohr) and weights, host arrays. The orbital basis is the plan's. Computes
- * S, T, V, the nuclear repulsion and the canonical orthonormalizer (device).
- * Replaces KS.__init__'s non-DF part (energy.py:549-654) and scf.py:73-90. */
+ * S, T, V, the nuclear repulsion and the canonical orthonormalizer (device)
+ * on `stream`, and returns with that work complete. Replaces KS.__init__'s
+ * non-DF part (energy.py:549-654) and scf.py:73-90. */
 dfjk_status dfscf_create(dfjk_plan* plan, int32_t natom, const double* atom_xyz,
                          const double* atom_charge, int64_t npoint, const double* grid_xyz,
                          const double* grid_w, int32_t nocc, const dfscf_options* opts,
-                         dfscf** scf);
+                         dfscf** scf, void* stream);
 dfjk_status dfscf_destroy(dfscf* scf);
 
 /* Runs the SCF from P0 (device nao x nao; NULL: the core-Hamiltonian guess,

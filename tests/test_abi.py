@@ -1,5 +1,5 @@
 """C ABI and host logic, no GPU needed: the library loads and exports every
-entry point include/dfjk.h and include/dfscf.h declare; the synthetic workloads are what the
+entry point include/dfjk.h, include/dfscf.h and include/dfbatch.h declare; the synthetic workloads are what the
 configs describe."""
 
 import ctypes
@@ -15,10 +15,10 @@ from dftax_b200 import _lib, systems
 
 def header_functions():
     names = set()
-    for h in ("dfjk.h", "dfscf.h"):
+    for h in ("dfjk.h", "dfscf.h", "dfbatch.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        names |= set(re.findall(r"\b((?:dfjk|dfscf)_[a-z0-9_]+)\s*\(", src))
+        names |= set(re.findall(r"\b((?:dfjk|dfscf|dfbatch)_[a-z0-9_]+)\s*\(", src))
     return names
 
 
@@ -107,6 +107,35 @@ def test_scf_default_options():
 
 def test_scf_null_arguments_are_rejected():
     lib = _lib.load()
-    assert lib.dfscf_create(None, 0, None, None, 0, None, None, 0, None, None) == 1
+    assert lib.dfscf_create(None, 0, None, None, 0, None, None, 0, None, None, None) == 1
     assert lib.dfscf_run(None, None, None, None) == 1
     assert lib.dfscf_destroy(None) == 0
+
+
+def test_batch_estimate_grows_with_the_molecule():
+    """The admission estimate of a solve needs no device and grows with the
+    system: at least B (rows x fitted columns x 8 bytes) and the mixed form's
+    extra K digit planes."""
+    from dftax_b200.batch import make_request
+
+    lib = _lib.load()
+    est = {}
+    for name in ("water3", "water8"):
+        sym, xyz, orb, aux, nocc = systems.workload(name, seed=0)
+        for prec in ("fp64", "mixed"):
+            r, keep, nao = make_request(sym, xyz, orb, aux, precision=prec,
+                                        grid=(np.zeros((0, 3)), np.zeros(0)))
+            b = ctypes.c_int64()
+            assert lib.dfbatch_estimate(ctypes.byref(r), ctypes.byref(b)) == 0
+            est[name, prec] = b.value
+            assert b.value > (nao * (nao + 1) // 2) * aux.nao * 8
+    assert est["water8", "fp64"] > 2 * est["water3", "fp64"]
+    assert est["water8", "mixed"] > est["water8", "fp64"]
+
+
+def test_batch_null_arguments_are_rejected():
+    lib = _lib.load()
+    assert lib.dfbatch_create(0, None, None) == 1
+    assert lib.dfbatch_submit(None, None, None) == 1
+    assert lib.dfbatch_wait(None, 0, None) == 1
+    assert lib.dfbatch_destroy(None) == 0
