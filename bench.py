@@ -56,6 +56,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scf-steps", type=int, default=2,
                     help="timed SCF solves per precision (0: no SCF measurement)")
+    ap.add_argument("--serve-requests", type=int, default=16,
+                    help="requests of the seeded Poisson serving stream (0: none)")
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
+    ap.add_argument("--serve-max-water", type=int, default=12,
+                    help="largest water cluster of the stream (log-uniform from 3)")
+    ap.add_argument("--serve-max-alkane", type=int, default=8,
+                    help="largest alkane of the stream (log-uniform from 4)")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="also solve a batch of this many water clusters (64: the 64-cluster "
+                         "batch, n log-uniform in [3, 40])")
+    ap.add_argument("--workers", type=int, default=4, help="concurrent solves of the engine")
     ap.add_argument("--screen", type=float, default=0.0,
                     help="relative Schwarz screen of shell pairs (0: none, the default)")
     return ap.parse_args()
@@ -459,6 +470,10 @@ def run_ours(args, rank, world, local_rank):
             "energy": "DFCoulomb energy of P = 2 C C^T with a_x = 0.25 (PBE0 exchange share)"}
     if args.scf_steps > 0:
         line["scf"] = scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks)
+    if args.serve_requests > 0:
+        line["serve"] = serve_measure(args, precs, rank)
+    if args.batch > 0:
+        line["batch"] = batch_measure(args, precs, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         secs, parts, n = cpu_full_builds(args.workload, 1)
         line["cpu_baseline"] = {"value": round(1.0 / secs[0], 6), "unit": UNIT, "cores": n,
@@ -517,6 +532,123 @@ def scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks):
         line["fp64"] = out["fp64"]
         line["speedup_vs_fp64"] = round(out["fp64"]["ms_per_solve"] / out[head]["ms_per_solve"], 3)
         line["abs_dE_vs_fp64_Ha"] = abs(res[head].e_tot - res["fp64"].e_tot)
+    return line
+
+
+def _loguniform_ints(rng, lo, hi, n):
+    return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), n))).astype(int)
+
+
+def _requests(eng, mols, grids, prec):
+    return [eng.request(s, x, o, a, grid=g, precision=prec) for (s, x, o, a), g in zip(mols, grids)]
+
+
+def serve_measure(args, precs, rank):
+    """A seeded Poisson stream of SCF requests (water clusters, n log-uniform
+    in [3, serve-max-water], and alkanes, n log-uniform in [4, serve-max-alkane],
+    half each) through the batch engine: each request is submitted at its
+    arrival time while earlier ones run, admitted FIFO as device memory frees
+    up. Solves/s = requests / (last completion - first arrival); latency =
+    completion - arrival. Grids (Becke 75 x 302) are built before the stream
+    starts. The same stream is replayed per precision."""
+    from dftax_b200 import systems
+    from dftax_b200.batch import BatchEngine
+    from dftax_b200.grid import becke_grid
+
+    rng = np.random.default_rng(50 + rank)
+    n = args.serve_requests
+    kinds = rng.integers(0, 2, n)
+    wn = _loguniform_ints(rng, 3, args.serve_max_water, n)
+    an = _loguniform_ints(rng, 4, args.serve_max_alkane, n)
+    gaps = rng.exponential(1.0 / args.serve_rate, n)
+    mols, names = [], []
+    for i in range(n):
+        name = f"water{wn[i]}" if kinds[i] == 0 else f"alkane{an[i]}"
+        sym, xyz, orb, aux, _ = systems.workload(name, seed=1000 + i)
+        mols.append((sym, xyz, orb, aux))
+        names.append(name)
+    grids = [becke_grid(m[0], m[1]) for m in mols]
+    out, energies, ok_mask = {}, {}, {}
+    for prec in precs:
+        with BatchEngine(workers=args.workers) as eng:
+            reqs = _requests(eng, mols, grids, prec)
+            ids = []
+            t0 = time.perf_counter()
+            for i, req in enumerate(reqs):
+                due = t0 + float(np.sum(gaps[:i]))
+                time.sleep(max(0.0, due - time.perf_counter()))
+                ids.append(eng.submit_request(req))
+            res = [eng.wait(i) for i in ids]
+        ok = [r for r in res if r.status == 0]
+        lat = np.array([r.latency for r in ok])
+        span = max(r.t_end for r in ok) - min(r.t_submit for r in ok)
+        energies[prec] = [r.e_tot for r in res]
+        ok_mask[prec] = [r.status == 0 for r in res]
+        out[prec] = {"value": round(len(ok) / span, 4), "unit": "SCF solves/s",
+                     "p50_latency_s": round(float(np.percentile(lat, 50)), 3),
+                     "p99_latency_s": round(float(np.percentile(lat, 99)), 3),
+                     "failed": len(res) - len(ok),
+                     "failures": [{"molecule": names[i], "status": r.status,
+                                   "message": r.message[:160]}
+                                  for i, r in enumerate(res) if r.status != 0][:4],
+                     "converged": int(sum(r.converged for r in ok)),
+                     "max_concurrent": max(sum(1 for q in res if q.t_start <= r.t_start < q.t_end)
+                                           for r in res)}
+    head = precs[0]
+    line = dict(out[head])
+    line["precision"] = head
+    line["stream"] = {"requests": n, "rate_per_s": args.serve_rate, "workers": args.workers,
+                      "water_n": [3, args.serve_max_water], "alkane_n": [4, args.serve_max_alkane],
+                      "molecules": names, "seed": 50 + rank,
+                      "what": "closed-shell DF-PBE0 SCF per request, Becke 75 x 302 grid"}
+    if "fp64" in out and head != "fp64":
+        line["fp64"] = out["fp64"]
+        both = [i for i in range(n) if ok_mask[head][i] and ok_mask["fp64"][i]]
+        line["max_abs_dE_vs_fp64_Ha"] = (float(np.max(np.abs(
+            np.array(energies[head])[both] - np.array(energies["fp64"])[both]))) if both else None)
+    return line
+
+
+def batch_measure(args, precs, rank):
+    """A batch of water clusters, n log-uniform in [3, 40] (seeded), all
+    submitted at once to the batch engine: solves/s = clusters / (last
+    completion - first submission), per-molecule |dE| of the headline precision
+    against float64."""
+    from dftax_b200 import systems
+    from dftax_b200.batch import BatchEngine
+    from dftax_b200.grid import becke_grid
+
+    rng = np.random.default_rng(64 + rank)
+    ns = _loguniform_ints(rng, 3, 40, args.batch)
+    mols = []
+    for i, n in enumerate(ns):
+        sym, xyz, orb, aux, _ = systems.workload(f"water{n}", seed=2000 + i)
+        mols.append((sym, xyz, orb, aux))
+    grids = [becke_grid(m[0], m[1]) for m in mols]
+    out, energies = {}, {}
+    for prec in precs:
+        with BatchEngine(workers=args.workers) as eng:
+            t0 = time.perf_counter()
+            ids = [eng.submit(*m, grid=g, precision=prec) for m, g in zip(mols, grids)]
+            res = [eng.wait(i) for i in ids]
+            sec = time.perf_counter() - t0
+        energies[prec] = np.array([r.e_tot for r in res])
+        out[prec] = {"value": round(len(res) / sec, 4), "unit": "SCF solves/s",
+                     "seconds": round(sec, 2),
+                     "failed": int(sum(r.status != 0 for r in res)),
+                     "failures": [{"n": int(ns[i]), "status": r.status, "message": r.message[:160]}
+                                  for i, r in enumerate(res) if r.status != 0][:4],
+                     "converged": int(sum(r.converged for r in res))}
+    head = precs[0]
+    line = dict(out[head])
+    line["precision"] = head
+    line["clusters"] = {"count": int(args.batch), "n": ns.tolist(), "seed": 64 + rank,
+                        "workers": args.workers}
+    if "fp64" in out and head != "fp64":
+        line["fp64"] = out["fp64"]
+        d = np.abs(energies[head] - energies["fp64"])
+        line["abs_dE_vs_fp64_Ha"] = {"max": float(d.max()), "median": float(np.median(d)),
+                                     "all_below_1uHa": bool(np.all(d < 1e-6))}
     return line
 
 

@@ -73,7 +73,13 @@ class BatchEngine:
         return b.value
 
     def submit(self, symbols, coords_bohr, orb, aux, *, want_density=False, **kw) -> int:
-        r, keep, nao = self.request(symbols, coords_bohr, orb, aux, **kw)
+        req = self.request(symbols, coords_bohr, orb, aux, **kw)
+        return self.submit_request(req, want_density=want_density)
+
+    def submit_request(self, req, *, want_density=False) -> int:
+        """Submit a request made by ``request``/``make_request`` (its arrays
+        are copied by the engine)."""
+        r, keep, nao = req
         P = np.empty((nao, nao)) if want_density else None
         r.P_out = P.ctypes.data if P is not None else None
         jid = ctypes.c_int64()

@@ -30,9 +30,10 @@ void fail(dfjk_status code, const char* fmt, ...) {
 // cudaMalloc of tens of GB plus cudaFree (which synchronizes the device) cost
 // ~100 ms per (H2O)_32 plan. Freed buffers are kept per device and handed out
 // again to requests of at most their size and at least 3/4 of it. A cached
-// buffer may still be read by work queued before it was freed, so reusing it
-// first synchronizes the device, unless the device was synchronized after the
-// buffer was freed (epoch). A failed cudaMalloc empties the cache and retries;
+// buffer may still be used by work queued before it was freed (on any stream,
+// by any thread), so every free takes a sequence number, and a reuse first
+// synchronizes the device unless a device synchronization that began after
+// the free has completed. A failed cudaMalloc empties the cache and retries;
 // dfjk_trim empties it on request.
 // ---------------------------------------------------------------------------
 
@@ -40,7 +41,7 @@ namespace {
 struct Cached {
   void* p;
   size_t bytes;
-  uint64_t epoch;
+  uint64_t stamp;   // sequence number of the free
 };
 std::mutex g_cache_mu;
 // never destroyed: cudaFree at process exit could run after the driver shut down
@@ -48,7 +49,12 @@ std::vector<std::vector<Cached>>& cache() {
   static auto* c = new std::vector<std::vector<Cached>>(64);
   return *c;
 }
-std::vector<uint64_t>& epochs() {
+// per device: the last sequence number handed out, and the largest one known idle
+std::vector<uint64_t>& free_seq() {
+  static auto* e = new std::vector<uint64_t>(64, 0);
+  return *e;
+}
+std::vector<uint64_t>& idle_upto() {
   static auto* e = new std::vector<uint64_t>(64, 0);
   return *e;
 }
@@ -67,20 +73,23 @@ void* cache_take(int dev, size_t n, size_t* got) {
     if (best == v.size()) return nullptr;
     p = v[best].p;
     *got = v[best].bytes;
-    need_sync = v[best].epoch == epochs()[dev];
+    need_sync = v[best].stamp > idle_upto()[dev];
     v.erase(v.begin() + best);
   }
-  if (need_sync) {
-    DFJK_CUDA(cudaDeviceSynchronize());
-    device_synchronized(dev);
-  }
+  if (need_sync) sync_device(dev);
   return p;
 }
 }  // namespace
 
-void device_synchronized(int dev) {
+void sync_device(int dev) {
+  uint64_t s0;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    s0 = free_seq()[dev];
+  }
+  DFJK_CUDA(cudaDeviceSynchronize());
   std::lock_guard<std::mutex> lk(g_cache_mu);
-  if (dev >= 0 && dev < (int)epochs().size()) epochs()[dev]++;
+  idle_upto()[dev] = std::max(idle_upto()[dev], s0);
 }
 
 void cache_trim(int dev) {
@@ -159,7 +168,7 @@ void PhaseTimer::destroy() {
 void DevBuf::free() {
   if (p) {
     std::lock_guard<std::mutex> lk(g_cache_mu);
-    cache()[dev].push_back({p, bytes, epochs()[dev]});
+    cache()[dev].push_back({p, bytes, ++free_seq()[dev]});
   }
   p = nullptr;
   bytes = 0;
@@ -1010,13 +1019,12 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
 dfjk_status dfjk_plan_destroy(dfjk_plan* pl) {
   if (!pl) return DFJK_OK;
   if (pl->p.owned_by_parent) return DFJK_ERR_INVALID;   // freed with its parent
-  const int dev = pl->p.ctx->device;
-  cudaSetDevice(dev);
-  // work queued on the plan's buffers ends here; they go back to the cache idle
-  cudaDeviceSynchronize();
+  cudaSetDevice(pl->p.ctx->device);
+  // the buffers go back to the cache without a device synchronization: work
+  // still queued on them (on this or another stream) is waited for when a
+  // buffer is handed out again, so solves on other streams keep running
   delete pl->p.lr;
   delete pl;
-  dfjk::device_synchronized(dev);
   return DFJK_OK;
 }
 

@@ -71,7 +71,9 @@ struct Error {
   } while (0)
 
 // Device memory cache (api.cu): freed DevBufs are kept for reuse per device.
-void device_synchronized(int dev);   // after a cudaDeviceSynchronize on dev
+// Synchronizes device dev and records that every buffer freed before the
+// synchronization began is idle (may be handed out again without waiting).
+void sync_device(int dev);
 void cache_trim(int dev);            // cudaFree every cached buffer of dev
 
 // Device buffer owned by a plan or context (allocated through the cache).

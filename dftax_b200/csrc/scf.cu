@@ -322,14 +322,17 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
       f.B[(size_t)j * md + slot] = row[j];
     }
     std::vector<double> coef = diis_solve(f.B, count, md);
-    // F_ext = sum_i c_i F_i
+    // F_ext = sum_i c_i F_i over the filled slots 0 .. count-1 only: the
+    // others hold whatever the recycled buffer held, and 0 times a NaN
+    // pattern is NaN
     f.vec.ensure((size_t)md * sizeof(double));
-    DFJK_CUDA(cudaMemcpyAsync(f.vec.p, coef.data(), md * sizeof(double), cudaMemcpyHostToDevice, s));
+    DFJK_CUDA(cudaMemcpyAsync(f.vec.p, coef.data(), count * sizeof(double), cudaMemcpyHostToDevice,
+                              s));
     {
       const double one = 1.0, zero = 0.0;
       DFJK_CUBLAS(cublasSetStream(c.cublas, s));
-      DFJK_CUBLAS(cublasDgemv(c.cublas, CUBLAS_OP_N, (int)nn, md, &one, f.dF.as<double>(), (int)nn,
-                              f.vec.as<double>(), 1, &zero, f.A2.as<double>(), 1));
+      DFJK_CUBLAS(cublasDgemv(c.cublas, CUBLAS_OP_N, (int)nn, count, &one, f.dF.as<double>(),
+                              (int)nn, f.vec.as<double>(), 1, &zero, f.A2.as<double>(), 1));
     }
     double* Fext = f.A2.as<double>();
     if (f.o.level_shift != 0.0) {
@@ -483,6 +486,7 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     f->dF.alloc((size_t)f->o.diis_space * nn * sizeof(double));
     f->dE.alloc((size_t)f->o.diis_space * m * m * sizeof(double));
     DFJK_CUDA(cudaMemsetAsync(f->dE.p, 0, (size_t)f->o.diis_space * m * m * sizeof(double), s));
+    DFJK_CUDA(cudaMemsetAsync(f->dF.p, 0, (size_t)f->o.diis_space * nn * sizeof(double), s));
     DFJK_CUDA(cudaStreamSynchronize(s));
   });
   if (st != DFJK_OK) {

@@ -145,3 +145,28 @@ def test_poisson_stream_matches_solo(solo, grid):
         lat.append(r.latency)
     assert np.percentile(lat, 50) <= np.percentile(lat, 99)
     assert _overlaps([r for _, r in res])
+
+
+def test_stream_with_buffer_reuse_across_workers(grid):
+    """Alkanes (carbon f shells) and water clusters, each twice, four workers:
+    the device buffers of finished solves are reused by solves on other
+    streams while work is still queued. Every result is the solo result."""
+    from dftax_b200 import df, systems
+    from dftax_b200.batch import BatchEngine
+    from dftax_b200.ks import KS, scf
+
+    names = ["alkane4", "water5", "alkane6", "water3", "alkane5", "water4"]
+    mols = [systems.workload(nm, seed=7)[:4] for nm in names]
+    solo = []
+    for sym, xyz, orb, aux in mols:
+        ks = KS(sym, xyz, orb, coulomb=df(aux, precision="mixed"), grid=grid)
+        solo.append(scf(ks).e_tot)
+        ks.close()
+        ks.plan.close()
+    order = [0, 1, 2, 3, 4, 5, 2, 0, 5, 1, 4, 3]
+    with BatchEngine(workers=4) as eng:
+        ids = [(k, eng.submit(*mols[k], grid=grid, precision="mixed")) for k in order]
+        res = [(k, eng.wait(i)) for k, i in ids]
+    for k, r in res:
+        assert r.status == 0, (names[k], r.message)
+        assert abs(r.e_tot - solo[k]) < E_TOL, names[k]
