@@ -83,7 +83,8 @@ class ScfResult(ctypes.Structure):
                 ("e_xc", c_double), ("e_nn", c_double), ("derr", c_double),
                 ("n_iter", c_int32), ("converged", c_int32), ("nmo", c_int32),
                 ("nocc", c_int32), ("ms_jk", c_double), ("ms_xc", c_double),
-                ("ms_diag", c_double), ("ms_diis", c_double)]
+                ("ms_diag", c_double), ("ms_diis", c_double), ("xc_chunk", c_int64),
+                ("xc_graph", c_int32), ("reserved", c_int32)]
 
 
 class BatchOptions(ctypes.Structure):

@@ -27,6 +27,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <map>
+#include <mutex>
 
 namespace dfjk {
 double energy(Plan& p, const double* P, int nspin, double hf, double hf_lr, double* F,
@@ -49,6 +51,7 @@ struct dfscf {
   std::vector<double> B;   // DIIS error overlaps, m x m
   dfscf_result res{};
   bool have_orbitals = false;
+  int64_t tuned_chunk = 0;   // XC points per chunk chosen by the autotuner (0: not tuned)
 };
 
 namespace dfjk {
@@ -355,8 +358,61 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
   }
   f.res.e_tot = e_prev;
   f.res.derr = derr;
+  f.res.xc_chunk = f.xcw.ch.G;
+  f.res.xc_graph = f.xcw.exec != nullptr ? 1 : 0;
   f.res.n_iter = it;
   f.res.converged = converged ? 1 : 0;
+}
+
+// Points per XC chunk, chosen by timing: the chunk size sets the shapes of the
+// two DGEMMs per chunk (G x nsig x nsig) and the launches per evaluation.
+// Candidates 4096, 8192 and 16384 points are timed on the core-guess density
+// (two evaluations each, the second timed, launched directly) for the first
+// molecule of each (nao / 128, log2 points) bucket; the choice is kept for
+// the process, so later molecules of that size (solves in a batch included)
+// use it without timing.
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, int64_t>& tuned() {
+  static auto* m = new std::map<std::pair<int, int>, int64_t>();
+  return *m;
+}
+
+void autotune_chunk(dfscf& f, const int (&nout)[8], const std::vector<double>& pv,
+                    cudaStream_t s) {
+  int lg = 0;
+  while ((int64_t(1) << (lg + 1)) <= f.npts) ++lg;
+  const std::pair<int, int> key{(f.nao + 127) / 128, lg};
+  int64_t best = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = tuned().find(key);
+    if (it != tuned().end()) best = it->second;
+  }
+  if (best == 0) {
+    make_density(f, f.H.as<double>(), s);   // core-guess density to time on
+    double best_ms = INFINITY;
+    f.xcw.graph_off = true;
+    for (int64_t G : {4096, 8192, 16384}) {
+      if ((int64_t)6 * f.nao * G * 8 > ((int64_t)3 << 30)) continue;
+      xc_chunk(f.p->orb, nout, pv, G, f.o.ao_thresh, f.xcw);
+      xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),
+                     f.Vxc.as<double>(), xc_params(f), f.xcw, s);
+      const auto t0 = std::chrono::steady_clock::now();
+      xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),
+                     f.Vxc.as<double>(), xc_params(f), f.xcw, s);
+      const double ms =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = G;
+      }
+    }
+    f.xcw.graph_off = false;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tuned().emplace(key, best);
+  }
+  f.tuned_chunk = best;
+  xc_chunk(f.p->orb, nout, pv, best, f.o.ao_thresh, f.xcw);   // also a fresh graph state
 }
 
 }  // namespace
@@ -418,13 +474,16 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     upload(f->atom_xyz, std::vector<double>(atom_xyz, atom_xyz + 3 * natom));
     upload(f->atom_z, std::vector<double>(atom_charge, atom_charge + natom));
     if (!(f->o.ao_thresh >= 0.0)) fail(DFJK_ERR_INVALID, "ao_thresh must be >= 0");
+    std::vector<double> pv, wv;
+    int nout[8];
+    for (int l = 0; l < 8; ++l) nout[l] = p.orb.spherical ? 2 * l + 1 : ncart(l);
     if (npoint > 0) {
       // spatially sorted chunks with their non-negligible shells
-      std::vector<double> pv(grid_xyz, grid_xyz + 3 * npoint), wv(grid_w, grid_w + npoint);
+      pv.assign(grid_xyz, grid_xyz + 3 * npoint);
+      wv.assign(grid_w, grid_w + npoint);
+      xc_sort(pv, wv);
       const int64_t G = f->o.grid_chunk > 0 ? (f->o.grid_chunk + 255) / 256 * 256 : 8192;
-      int nout[8];
-      for (int l = 0; l < 8; ++l) nout[l] = p.orb.spherical ? 2 * l + 1 : ncart(l);
-      xc_prepare(p.orb, nout, pv, wv, G, f->o.ao_thresh, f->xcw.ch);
+      xc_chunk(p.orb, nout, pv, G, f->o.ao_thresh, f->xcw);
       upload(f->pts, pv);
       upload(f->wts, wv);
     }
@@ -487,6 +546,7 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     f->dE.alloc((size_t)f->o.diis_space * m * m * sizeof(double));
     DFJK_CUDA(cudaMemsetAsync(f->dE.p, 0, (size_t)f->o.diis_space * m * m * sizeof(double), s));
     DFJK_CUDA(cudaMemsetAsync(f->dF.p, 0, (size_t)f->o.diis_space * nn * sizeof(double), s));
+    if (npoint > 0 && f->o.grid_chunk <= 0 && has_xc(*f)) autotune_chunk(*f, nout, pv, s);
     DFJK_CUDA(cudaStreamSynchronize(s));
   });
   if (st != DFJK_OK) {

@@ -43,14 +43,29 @@ struct XcWork {
   DevBuf phi, dphi, X, W;       // [nsig][G] AO values, 3 gradients, Phi P, weighted AO
   DevBuf Pc, Vc, Vacc;          // P on a chunk's AOs, its V block, V accumulated
   DevBuf vr, vg, ered;          // per point: v_rho, v_grad (3), energy partials per block
+  // the evaluation's device work as a CUDA graph, captured on the second call
+  // with the same arguments and replayed while they stay the same
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cap = nullptr;   // private stream the work is captured on (capture only
+                                // records; the graph is launched on the caller's stream)
+  const void* g_args[4] = {nullptr, nullptr, nullptr, nullptr};   // P, Vxc, pts, w
+  int64_t graph_kernels = 0;    // this library's kernels in the graph
+  int calls = 0;
+  bool graph_off = false;       // capture failed once: run the launches directly
+  ~XcWork() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (cap) cudaStreamDestroy(cap);
+  }
 };
 
-// Sorts the points (and weights) along a Morton curve over 1-Bohr cells, cuts
-// them into chunks of G points and keeps for each chunk the shells whose
-// value-and-gradient bound over the chunk's bounding box exceeds thresh.
+// Sorts the points (and weights) along a Morton curve over 1-Bohr cells;
 // pts [n][3] and w [n] are host arrays, reordered in place.
-void xc_prepare(const Shells& sh, const int (&nout)[8], std::vector<double>& pts,
-                std::vector<double>& w, int64_t G, double thresh, XcChunks& out);
+void xc_sort(std::vector<double>& pts, std::vector<double>& w);
+// Cuts sorted points into chunks of G points and keeps for each chunk the
+// shells whose value-and-gradient bound over the chunk's bounding box exceeds
+// thresh (uploads the shell lists); forgets any captured graph of ws.
+void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>& pts, int64_t G,
+              double thresh, XcWork& ws);
 
 struct XcParams {
   double x_scale = 0.75;        // PBE exchange share (PBE0)

@@ -15,7 +15,9 @@
 //   W = v_rho/2 Phi + v_grad . dPhi, V += Phi^T W               (cuBLAS DGEMM);
 // and at the end Vxc = V + V^T, the symmetrized P-gradient of E_xc
 // (scf.py:42-46). The energy is summed per block in a fixed order and then
-// over blocks on the host, so it is reproducible.
+// over blocks on the host, so it is reproducible. The SCF calls this with
+// the same buffers every iteration: the second call captures its launches
+// (about eight per chunk) in a CUDA graph and later calls replay it.
 #include "scf.h"
 
 #include <algorithm>
@@ -389,18 +391,8 @@ static uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
   return spread(x) | spread(y) << 1 | spread(z) << 2;
 }
 
-void xc_prepare(const Shells& sh, const int (&nout)[8], std::vector<double>& pts,
-                std::vector<double>& w, int64_t G, double thresh, XcChunks& out) {
+void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
   const int64_t n = (int64_t)w.size();
-  out.g0.clear();
-  out.ng.clear();
-  out.sh_off.clear();
-  out.sh_cnt.clear();
-  out.ao_off.clear();
-  out.ao_cnt.clear();
-  out.max_ao = 0;
-  out.total_ao = 0;
-  out.G = G;
   if (n == 0) return;
   // Morton order of 1-Bohr cells
   double lo[3] = {INFINITY, INFINITY, INFINITY};
@@ -421,9 +413,30 @@ void xc_prepare(const Shells& sh, const int (&nout)[8], std::vector<double>& pts
   }
   pts.swap(p2);
   w.swap(w2);
+}
+
+void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>& pts, int64_t G,
+              double thresh, XcWork& ws) {
+  XcChunks& out = ws.ch;
+  const int64_t n = (int64_t)pts.size() / 3;
+  out.g0.clear();
+  out.ng.clear();
+  out.sh_off.clear();
+  out.sh_cnt.clear();
+  out.ao_off.clear();
+  out.ao_cnt.clear();
+  out.max_ao = 0;
+  out.total_ao = 0;
+  out.G = G;
+  if (ws.exec) cudaGraphExecDestroy(ws.exec);
+  ws.exec = nullptr;
+  for (auto& a : ws.g_args) a = nullptr;
+  ws.calls = 0;
+  if (n == 0) return;
   // per shell: |phi| + |grad phi| <= sum_k |c_k| (1 + r^l + l r^(l-1) + 2 a_k r^(l+1)) e^(-a_k r^2)
-  // for r beyond the distance d from the shell to a box, each term taken at
-  // max(d, its peak) (the factors decrease past sqrt((l+1)/(2 a_k)))
+  // for r beyond the distance d from the shell to a box, the polynomial taken
+  // at max(d, its peak) (it decreases past sqrt((l+1)/(2 a_k))) and the
+  // Gaussian at d
   auto bound = [&](int s, double d) {
     const int l = sh.l[s];
     double b = 0.0;
@@ -431,8 +444,7 @@ void xc_prepare(const Shells& sh, const int (&nout)[8], std::vector<double>& pts
       const double a = sh.pexp[sh.prim0[s] + k], c = std::fabs(sh.pcoef[sh.prim0[s] + k]);
       const double r = std::max(d, std::sqrt((l + 1) / (2.0 * a)));
       const double rl = std::pow(r, l);
-      b += c * (1.0 + rl + (l > 0 ? l * rl / r : 0.0) + 2.0 * a * rl * r) *
-           std::exp(-a * std::max(d, 0.0) * std::max(d, 0.0));
+      b += c * (1.0 + rl + (l > 0 ? l * rl / r : 0.0) + 2.0 * a * rl * r) * std::exp(-a * d * d);
     }
     return b;
   };
@@ -474,29 +486,17 @@ void xc_prepare(const Shells& sh, const int (&nout)[8], std::vector<double>& pts
   upload(out.d_ao_map, aomap);
 }
 
-double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, const double* w,
-                      const double* P, double* Vxc, const XcParams& xp, XcWork& ws,
-                      cudaStream_t s) {
+// enqueues one evaluation's device work on s (buffers already sized)
+static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, const double* w,
+                       const double* P, double* Vxc, const XcParams& xp, XcWork& ws,
+                       cudaStream_t s) {
   const int nao = ov.nao;
   const XcChunks& ch = ws.ch;
   const int64_t G = ch.G;
   const int64_t nchunk = (int64_t)ch.g0.size();
   const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
-  const int64_t plane_max = (int64_t)std::max(ch.max_ao, 1) * G;
-  ws.phi.ensure(plane_max * sizeof(double));
-  ws.dphi.ensure(3 * plane_max * sizeof(double));
-  ws.X.ensure(plane_max * sizeof(double));
-  ws.W.ensure(plane_max * sizeof(double));
-  ws.Pc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
-  ws.Vc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
-  ws.vr.ensure(G * sizeof(double));
-  ws.vg.ensure(3 * G * sizeof(double));
-  ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
-  if (Vxc) {
-    ws.Vacc.ensure((size_t)nao * nao * sizeof(double));
-    DFJK_CUDA(cudaMemsetAsync(ws.Vacc.p, 0, (size_t)nao * nao * sizeof(double), s));
-  }
+  if (Vxc) DFJK_CUDA(cudaMemsetAsync(ws.Vacc.p, 0, (size_t)nao * nao * sizeof(double), s));
   const double one = 1.0, zero = 0.0;
   for (int64_t k = 0; k < nchunk; ++k) {
     const int64_t g0 = ch.g0[k], ng = ch.ng[k];
@@ -546,6 +546,69 @@ double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, co
                                                                         Vxc);
     DFJK_LAUNCHED();
   }
+}
+
+double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, const double* w,
+                      const double* P, double* Vxc, const XcParams& xp, XcWork& ws,
+                      cudaStream_t s) {
+  const int nao = ov.nao;
+  const XcChunks& ch = ws.ch;
+  const int64_t G = ch.G;
+  const int64_t nchunk = (int64_t)ch.g0.size();
+  const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
+  const int64_t plane_max = (int64_t)std::max(ch.max_ao, 1) * G;
+  ws.phi.ensure(plane_max * sizeof(double));
+  ws.dphi.ensure(3 * plane_max * sizeof(double));
+  ws.X.ensure(plane_max * sizeof(double));
+  ws.W.ensure(plane_max * sizeof(double));
+  ws.Pc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
+  ws.Vc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
+  ws.vr.ensure(G * sizeof(double));
+  ws.vg.ensure(3 * G * sizeof(double));
+  ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
+  if (Vxc) ws.Vacc.ensure((size_t)nao * nao * sizeof(double));
+  const void* args[4] = {P, Vxc, pts, w};
+  const bool same = std::equal(args, args + 4, ws.g_args);
+  if (ws.exec && same) {
+    DFJK_CUDA(cudaGraphLaunch(ws.exec, s));
+    count_launch(ws.graph_kernels);
+  } else if (!ws.graph_off && ws.calls > 0 && Vxc) {
+    // capture this call's work (the buffers above are already sized, and the
+    // first, direct call let cuBLAS set up its workspace outside capture)
+    if (ws.exec) {
+      DFJK_CUDA(cudaGraphExecDestroy(ws.exec));
+      ws.exec = nullptr;
+    }
+    if (!ws.cap) DFJK_CUDA(cudaStreamCreateWithFlags(&ws.cap, cudaStreamNonBlocking));
+    const int64_t k0 = dfjk_kernel_launches();
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(ws.cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      try {
+        xc_enqueue(c, ov, pts, w, P, Vxc, xp, ws, ws.cap);
+      } catch (...) {
+        ok = false;
+      }
+      const cudaError_t ec = cudaStreamEndCapture(ws.cap, &graph);
+      ok = ok && ec == cudaSuccess && graph;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ws.exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (ok) {
+      ws.graph_kernels = dfjk_kernel_launches() - k0;
+      std::copy(args, args + 4, ws.g_args);
+      DFJK_CUDA(cudaGraphLaunch(ws.exec, s));
+    } else {
+      // the same kernels, launched directly
+      ws.exec = nullptr;
+      ws.graph_off = true;
+      xc_enqueue(c, ov, pts, w, P, Vxc, xp, ws, s);
+    }
+  } else {
+    xc_enqueue(c, ov, pts, w, P, Vxc, xp, ws, s);
+  }
+  ++ws.calls;
   std::vector<double> e((size_t)nchunk * nblk);
   if (!e.empty())
     DFJK_CUDA(cudaMemcpyAsync(e.data(), ws.ered.p, e.size() * sizeof(double),

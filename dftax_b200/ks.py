@@ -49,6 +49,8 @@ class KSResult:
     e_xc: float = 0.0
     e_coul: float = 0.0
     timings_ms: dict | None = None   # J/K, XC, diagonalization, DIIS of the run
+    xc_chunk: int = 0                # grid points per XC chunk (set or autotuned)
+    xc_graph: bool = False           # XC evaluations replayed a captured CUDA graph
 
 
 class KS:
@@ -200,7 +202,8 @@ def scf(ks: KS, *, max_iter: int = 128, e_tol: float = 1e-8, d_tol: float = 1e-6
                     mo_coeff=C.T.cpu().numpy()[None], P=P.cpu().numpy()[None], e_xc=r.e_xc,
                     e_coul=r.e_coul,
                     timings_ms={"jk": r.ms_jk, "xc": r.ms_xc, "diag": r.ms_diag,
-                                "diis": r.ms_diis})
+                                "diis": r.ms_diis},
+                    xc_chunk=int(r.xc_chunk), xc_graph=bool(r.xc_graph))
 
 
 __all__ = ["KS", "KSResult", "scf", "XC_FUNCTIONALS"]

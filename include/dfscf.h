@@ -41,7 +41,9 @@ typedef struct {
                            every shell, the dense quadrature)                          */
   int32_t max_iter;     /* 128                                                          */
   int32_t diis_space;   /* DIIS history depth (8)                                        */
-  int64_t grid_chunk;   /* grid points per XC chunk, spatially sorted (0: 8192)         */
+  int64_t grid_chunk;   /* grid points per XC chunk, spatially sorted (0: chosen by
+                           timing 4096, 8192 and 16384 on the first molecule of each
+                           size; the choice is kept for the process)                   */
 } dfscf_options;
 
 typedef struct {
@@ -59,6 +61,9 @@ typedef struct {
    * synchronized device work): J and K, the XC quadrature, the Fock
    * diagonalizations with the density, the commutator and DIIS */
   double ms_jk, ms_xc, ms_diag, ms_diis;
+  int64_t xc_chunk;     /* grid points per XC chunk (set, or chosen by the autotuner)    */
+  int32_t xc_graph;     /* 1: the XC evaluations replayed a captured CUDA graph          */
+  int32_t reserved;
 } dfscf_result;
 
 /* dftax's defaults for PBE0 (scf.py:279-391, xc.py:584-601, grid.py:10-45). */
