@@ -18,6 +18,7 @@
 // over blocks on the host, so it is reproducible. The SCF calls this with
 // the same buffers every iteration: the second call captures its launches
 // (about eight per chunk) in a CUDA graph and later calls replay it.
+#include "md_device.cuh"
 #include "scf.h"
 
 #include <algorithm>
@@ -78,9 +79,85 @@ __device__ __forceinline__ double ipow(double x, int n) {
   return r;
 }
 
+// p[n] for 0 <= n <= L (p[0] for n < 0) by selects, so p stays in registers
+// whether or not n folds to a constant
+template <int L>
+__device__ __forceinline__ double pick(const double (&p)[L + 1], int n) {
+  double r = p[0];
+#pragma unroll
+  for (int i = 1; i <= L; ++i) r = n == i ? p[i] : r;
+  return r;
+}
+
+// values and gradients of one shell's NC cartesian components at (dx, dy,
+// dz), in dftax's order (lx descending, then ly), transformed by the shell's
+// block T (NC x nout) and stored at o, o + plane, ...; L is a template
+// parameter so the component arrays stay in registers
+template <int L>
+__device__ __forceinline__ void ao_shell(const OrbView& ov, int s, double dx, double dy,
+                                         double dz, bool live, int64_t o, int64_t G,
+                                         int64_t plane, double* __restrict__ phi,
+                                         double* __restrict__ dphi) {
+  constexpr int NC = (L + 1) * (L + 2) / 2;
+  const ShellView& sh = ov.sh;
+  const int nout = ov.nout[L];                 // constant index: no local copy of ov
+  const double* __restrict__ T = ov.c2s + ov.c2s_off[L];
+  double val[NC], gx[NC], gy[NC], gz[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) val[k] = gx[k] = gy[k] = gz[k] = 0.0;
+  if (live) {
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    double rad = 0.0, drad = 0.0;
+    for (int k = 0; k < sh.nprim[s]; ++k) {
+      const double a = sh.pexp[sh.prim0[s] + k], c = sh.pcoef[sh.prim0[s] + k];
+      const double e = c * exp(-a * r2);
+      rad += e;
+      drad += -2.0 * a * e;
+    }
+    double px[L + 1], py[L + 1], pz[L + 1];
+    px[0] = py[0] = pz[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k <= L; ++k) {
+      px[k] = px[k - 1] * dx;
+      py[k] = py[k - 1] * dy;
+      pz[k] = pz[k - 1] * dz;
+    }
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+      const int lx = comp_x(L, k), ly = comp_y(L, k), lz = L - lx - ly;
+      const double xl = pick<L>(px, lx), yl = pick<L>(py, ly), zl = pick<L>(pz, lz);
+      const double ang = xl * yl * zl;
+      val[k] = ang * rad;
+      const double dpx = lx * pick<L>(px, lx - 1);
+      const double dpy = ly * pick<L>(py, ly - 1);
+      const double dpz = lz * pick<L>(pz, lz - 1);
+      gx[k] = dpx * yl * zl * rad + ang * drad * dx;
+      gy[k] = xl * dpy * zl * rad + ang * drad * dy;
+      gz[k] = xl * yl * dpz * rad + ang * drad * dz;
+    }
+  }
+  for (int m = 0; m < nout; ++m) {
+    double v = 0.0, a = 0.0, b = 0.0, c = 0.0;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      const double t = T[q * nout + m];
+      v += val[q] * t;
+      a += gx[q] * t;
+      b += gy[q] * t;
+      c += gz[q] * t;
+    }
+    const int64_t om = o + (int64_t)m * G;
+    phi[om] = v;
+    dphi[om] = a;
+    dphi[plane + om] = b;
+    dphi[2 * plane + om] = c;
+  }
+}
+
 // Phi[k][g] (ld G), dPhi[x][k][g] for the chunk's shells: shell j of the
 // chunk is orbital shell sh[j] with compact AOs k = out0c[j] .. ; grid
-// (ceil(G / 128), shells of the chunk)
+// (ceil(G / 128), shells of the chunk); every thread of a block has the same
+// shell, so the switch on l is uniform
 __global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const int* __restrict__ shl,
                                                         const int* __restrict__ out0c,
                                                         const double* __restrict__ pts,
@@ -91,52 +168,22 @@ __global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const int* _
   const int s = shl[blockIdx.y];
   if (g >= G) return;
   const ShellView& sh = ov.sh;
-  const int l = sh.l[s], nc = (l + 1) * (l + 2) / 2, nout = ov.nout[l];
-  const int64_t mu0 = out0c[blockIdx.y];
+  const int l = sh.l[s];
+  const int64_t o = (int64_t)out0c[blockIdx.y] * G + g;
   const int64_t plane = (int64_t)nsig * G;
-  double val[10] = {}, gx[10] = {}, gy[10] = {}, gz[10] = {};
-  if (g < ng) {
+  const bool live = g < ng;
+  double dx = 0.0, dy = 0.0, dz = 0.0;
+  if (live) {
     const double* p = pts + 3 * (g0 + g);
-    const double dx = p[0] - sh.cen[3 * s], dy = p[1] - sh.cen[3 * s + 1],
-                 dz = p[2] - sh.cen[3 * s + 2];
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    double rad = 0.0, drad = 0.0;
-    for (int k = 0; k < sh.nprim[s]; ++k) {
-      const double a = sh.pexp[sh.prim0[s] + k], c = sh.pcoef[sh.prim0[s] + k];
-      const double e = c * exp(-a * r2);
-      rad += e;
-      drad += -2.0 * a * e;
-    }
-    int k = 0;
-    for (int lx = l; lx >= 0; --lx)
-      for (int ly = l - lx; ly >= 0; --ly, ++k) {
-        const int lz = l - lx - ly;
-        const double px_ = ipow(dx, lx), py_ = ipow(dy, ly), pz_ = ipow(dz, lz);
-        const double ang = px_ * py_ * pz_;
-        val[k] = ang * rad;
-        const double dpx = lx > 0 ? lx * ipow(dx, lx - 1) : 0.0;
-        const double dpy = ly > 0 ? ly * ipow(dy, ly - 1) : 0.0;
-        const double dpz = lz > 0 ? lz * ipow(dz, lz - 1) : 0.0;
-        gx[k] = dpx * py_ * pz_ * rad + ang * drad * dx;
-        gy[k] = px_ * dpy * pz_ * rad + ang * drad * dy;
-        gz[k] = px_ * py_ * dpz * rad + ang * drad * dz;
-      }
+    dx = p[0] - sh.cen[3 * s];
+    dy = p[1] - sh.cen[3 * s + 1];
+    dz = p[2] - sh.cen[3 * s + 2];
   }
-  const double* T = ov.c2s + ov.c2s_off[l];
-  for (int m = 0; m < nout; ++m) {
-    double v = 0.0, a = 0.0, b = 0.0, c = 0.0;
-    for (int q = 0; q < nc; ++q) {
-      const double t = T[q * nout + m];
-      v += val[q] * t;
-      a += gx[q] * t;
-      b += gy[q] * t;
-      c += gz[q] * t;
-    }
-    const int64_t o = (mu0 + m) * G + g;
-    phi[o] = v;
-    dphi[o] = a;
-    dphi[plane + o] = b;
-    dphi[2 * plane + o] = c;
+  switch (l) {
+    case 0: ao_shell<0>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
+    case 1: ao_shell<1>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
+    case 2: ao_shell<2>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
+    default: ao_shell<3>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
   }
 }
 
@@ -158,26 +205,41 @@ __global__ void scatter_v_kernel(const double* __restrict__ Vc, int nsig, const 
   V[(int64_t)map[b] * nao + map[a]] += Vc[i];
 }
 
-// rho[g] = sum_mu X Phi, grad[x][g] = 2 sum_mu X dPhi_x
-__global__ void rho_kernel(const double* __restrict__ X, const double* __restrict__ phi,
-                           const double* __restrict__ dphi, int nao, int64_t G, int64_t ng,
-                           double* __restrict__ rho, double* __restrict__ grad) {
-  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (g >= ng) return;
+// rho[g] = sum_mu X Phi, grad[x][g] = 2 sum_mu X dPhi_x. A block takes 32
+// points with 8 lanes of mu each (mu = lane, lane + 8, ...: a warp reads 32
+// consecutive points of one mu), and the 8 partial sums are added in a fixed
+// order, so the result does not depend on the launch.
+constexpr int kRhoPts = 32, kRhoLanes = 8;
+__global__ void __launch_bounds__(kRhoPts * kRhoLanes) rho_kernel(
+    const double* __restrict__ X, const double* __restrict__ phi, const double* __restrict__ dphi,
+    int nao, int64_t G, int64_t ng, double* __restrict__ rho, double* __restrict__ grad) {
+  __shared__ double red[4][kRhoLanes][kRhoPts];
+  const int gi = threadIdx.x % kRhoPts, ml = threadIdx.x / kRhoPts;
+  const int64_t g = blockIdx.x * (int64_t)kRhoPts + gi;
   const int64_t plane = (int64_t)nao * G;
   double r = 0.0, a = 0.0, b = 0.0, c = 0.0;
-  for (int mu = 0; mu < nao; ++mu) {
-    const int64_t o = (int64_t)mu * G + g;
-    const double x = X[o];
-    r += x * phi[o];
-    a += x * dphi[o];
-    b += x * dphi[plane + o];
-    c += x * dphi[2 * plane + o];
+  if (g < ng) {
+    for (int mu = ml; mu < nao; mu += kRhoLanes) {
+      const int64_t o = (int64_t)mu * G + g;
+      const double x = X[o];
+      r += x * phi[o];
+      a += x * dphi[o];
+      b += x * dphi[plane + o];
+      c += x * dphi[2 * plane + o];
+    }
   }
-  rho[g] = r;
-  grad[g] = 2.0 * a;
-  grad[G + g] = 2.0 * b;
-  grad[2 * G + g] = 2.0 * c;
+  red[0][ml][gi] = r;
+  red[1][ml][gi] = a;
+  red[2][ml][gi] = b;
+  red[3][ml][gi] = c;
+  __syncthreads();
+  if (ml < 4 && g < ng) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < kRhoLanes; ++q) t += red[ml][q][gi];
+    if (ml == 0) rho[g] = t;
+    else grad[(ml - 1) * G + g] = 2.0 * t;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -518,7 +580,7 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
     DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nsig, nsig, &one,
                             ws.phi.as<double>(), (int)G, ws.Pc.as<double>(), nsig, &zero,
                             ws.X.as<double>(), (int)G));
-    rho_kernel<<<(unsigned)((ng + kPtThreads - 1) / kPtThreads), kPtThreads, 0, s>>>(
+    rho_kernel<<<(unsigned)((ng + kRhoPts - 1) / kRhoPts), kRhoPts * kRhoLanes, 0, s>>>(
         ws.X.as<double>(), ws.phi.as<double>(), ws.dphi.as<double>(), nsig, G, ng,
         ws.vr.as<double>(), ws.vg.as<double>());
     DFJK_LAUNCHED();

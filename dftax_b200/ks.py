@@ -207,3 +207,40 @@ def scf(ks: KS, *, max_iter: int = 128, e_tol: float = 1e-8, d_tol: float = 1e-6
 
 
 __all__ = ["KS", "KSResult", "scf", "XC_FUNCTIONALS"]
+
+
+def _main(argv=None):
+    """``python -m dftax_b200.ks water8 --precision mixed``: one SCF solve of a
+    named workload (``systems.workload``) from geometry, printed as JSON."""
+    import argparse
+    import json
+    import time
+
+    from . import df, systems
+    from .grid import becke
+
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("workload")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--xc", default="PBE0", choices=sorted(XC_FUNCTIONALS))
+    ap.add_argument("--radial", type=int, default=75)
+    ap.add_argument("--lebedev", type=int, default=302)
+    ap.add_argument("--repeat", type=int, default=1, help="solves (the last one is reported)")
+    a = ap.parse_args(argv)
+    sym, xyz, orb, aux, nocc = systems.workload(a.workload, seed=0)
+    for _ in range(a.repeat):
+        t0 = time.perf_counter()
+        ks = KS(sym, xyz, orb, coulomb=df(aux, precision=a.precision), xc=a.xc,
+                grid=becke(a.radial, a.lebedev))
+        r = scf(ks)
+        sec = time.perf_counter() - t0
+        ks.close()
+        ks.plan.close()
+    print(json.dumps({"workload": a.workload, "precision": a.precision, "xc": a.xc,
+                      "e_tot": r.e_tot, "converged": r.converged, "n_iter": r.n_iter,
+                      "seconds": round(sec, 3), "parts_ms": r.timings_ms,
+                      "xc_chunk": r.xc_chunk, "xc_graph": r.xc_graph}))
+
+
+if __name__ == "__main__":
+    _main()
