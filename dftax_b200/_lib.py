@@ -16,6 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdfjk.so")
 
 DFJK_OK = 0
+(DFJK_ERR_INVALID, DFJK_ERR_UNSUPPORTED, DFJK_ERR_CUDA, DFJK_ERR_MEMORY, DFJK_ERR_NUMERIC,
+ DFJK_ERR_STATE) = range(1, 7)
 STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CUDA", 4: "MEMORY", 5: "NUMERIC",
                 6: "STATE"}
 DFJK_FP64 = 0
@@ -27,6 +29,7 @@ EXPORTS = (
     "dfjk_plan_create", "dfjk_plan_destroy", "dfjk_plan_get_info", "dfjk_build", "dfjk_jk",
     "dfjk_jk_host", "dfjk_energy", "dfjk_eri3c_dense", "dfjk_eri2c_dense", "dfjk_metric_pinv",
     "dfjk_kept_pairs", "dfjk_boys", "dfjk_phase_times", "dfjk_kernel_launches",
+    "dfjk_wait_selftest", "dfjk_energy_grad",
     "dfjk_j_noalloc", "dfjk_trim", "dfjk_plan_long_range", "dfjk_energy_rsh",
     # include/dfscf.h
     "dfscf_default_options", "dfscf_create", "dfscf_destroy", "dfscf_run", "dfscf_get_result",
@@ -60,7 +63,7 @@ class Basis(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("screen", c_double), ("metric_cutoff", c_double), ("precision", c_int32),
-                ("reserved", c_int32), ("chunk_bytes", c_int64), ("omega", c_double)]
+                ("streamed", c_int32), ("chunk_bytes", c_int64), ("omega", c_double)]
 
 
 class PlanInfo(ctypes.Structure):
@@ -137,6 +140,8 @@ def load(path: str | None = None):
         "dfjk_metric_pinv": (c_int, [V, V, V]),
         "dfjk_kept_pairs": (c_int, [V, V]),
         "dfjk_boys": (c_int, [V, V, c_int64, c_int32, V, V]),
+        "dfjk_wait_selftest": (c_int, [V, c_int64, V, V]),
+        "dfjk_energy_grad": (c_int, [V, V, c_int32, c_double, V, V, V, V]),
         "dfjk_phase_times": (c_int, [V, P(c_double), c_int32]),
         "dfjk_kernel_launches": (c_int64, []),
         "dfjk_j_noalloc": (c_int, [V, V, V, c_int64, V, V]),
@@ -181,4 +186,6 @@ def check(status: int, ctx=None):
 __all__ = ["load", "check", "Basis", "Options", "PlanInfo", "ScfOptions", "ScfResult",
            "BatchOptions", "BatchRequest", "BatchResult", "DfjkError",
            "LibraryNotLoaded",
-           "EXPORTS", "DFJK_FP64", "DFJK_MIXED", "byref"]
+           "EXPORTS", "DFJK_FP64", "DFJK_MIXED", "byref", "DFJK_OK", "DFJK_ERR_INVALID",
+           "DFJK_ERR_UNSUPPORTED", "DFJK_ERR_CUDA", "DFJK_ERR_MEMORY", "DFJK_ERR_NUMERIC",
+           "DFJK_ERR_STATE"]

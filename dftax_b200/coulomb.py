@@ -103,12 +103,34 @@ def _basis_struct(b: BasisData, keep: list):
 PRECISIONS = {"fp64": _lib.DFJK_FP64, "mixed": _lib.DFJK_MIXED}
 
 
+def shell_centers(b: BasisData) -> np.ndarray:
+    """(nshell, 3) centers of a basis's shells in the order the library reads
+    them: a shell starts at each cartesian row whose angular part is (l, 0, 0)."""
+    an = np.asarray(b.angular)
+    starts = np.nonzero((an[:, 1] == 0) & (an[:, 2] == 0))[0]
+    return np.asarray(b.centers, dtype=np.float64)[starts]
+
+
+def shells_to_atoms(shell_grad, centers, atom_xyz, tol: float = 1e-8) -> np.ndarray:
+    """Sum per-shell gradients (nshell, 3) onto the atoms whose positions
+    (natom, 3) the shell centers sit on."""
+    atom_xyz = np.asarray(atom_xyz, dtype=np.float64).reshape(-1, 3)
+    d = np.linalg.norm(np.asarray(centers)[:, None, :] - atom_xyz[None, :, :], axis=2)
+    idx = np.argmin(d, axis=1)
+    if len(idx) and d[np.arange(len(idx)), idx].max() > tol:
+        raise ValueError("a shell center is on no atom")
+    out = np.zeros_like(atom_xyz)
+    np.add.at(out, idx, np.asarray(shell_grad, dtype=np.float64))
+    return out
+
+
 class Plan:
     """One molecule's density-fitting plan on the device (``dfjk_plan``)."""
 
     def __init__(self, orb: BasisData, aux: BasisData, *, screen: float | None = None,
                  precision: str = "fp64", metric_cutoff: float = 1e-7, chunk_bytes: int = 0,
-                 omega: float = 0.0, device: int = 0, ctx: Context | None = None):
+                 omega: float = 0.0, streamed: bool = False, device: int = 0,
+                 ctx: Context | None = None):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         self.ctx = ctx or Context.get(device)
@@ -124,12 +146,15 @@ class Plan:
         opts.precision = PRECISIONS[precision]
         opts.chunk_bytes = int(chunk_bytes)
         opts.omega = float(omega)
+        opts.streamed = 1 if streamed else 0
         self.omega = float(omega)
+        self.streamed = bool(streamed)
         self._parent = None
         self.h = ctypes.c_void_p()
         check(self.lib.dfjk_plan_create(self.ctx.h, byref(ob), byref(ab), byref(opts),
                                         byref(self.h)), self.ctx.h)
         self.precision = precision
+        self.orb_centers, self.aux_centers = shell_centers(orb), shell_centers(aux)
 
     # -- lifecycle -------------------------------------------------------
     def close(self):
@@ -234,6 +259,27 @@ class Plan:
                                        _stream_ptr(t, stream)), self.ctx.h)
         return e.value, F
 
+    def energy_grad(self, P, hf_coeff: float, atom_xyz=None, *, stream=None):
+        """Energy and nuclear gradient of the DF energy at the fixed symmetric
+        density P (``dfjk_energy_grad``). With ``atom_xyz`` (natom, 3) the
+        gradient is summed per atom, (E, (natom, 3)); otherwise per shell,
+        (E, (norb_shell, 3), (naux_shell, 3))."""
+        t = self.torch
+        P = self._dev(P)
+        if P.ndim == 2:
+            P = P[None]
+        go = t.empty((len(self.orb_centers), 3), dtype=t.float64, device=self.dev)
+        ga = t.empty((len(self.aux_centers), 3), dtype=t.float64, device=self.dev)
+        e = ctypes.c_double()
+        check(self.lib.dfjk_energy_grad(self.h, P.data_ptr(), P.shape[0], float(hf_coeff),
+                                        byref(e), go.data_ptr(), ga.data_ptr(),
+                                        _stream_ptr(t, stream)), self.ctx.h)
+        go, ga = go.cpu().numpy(), ga.cpu().numpy()
+        if atom_xyz is None:
+            return e.value, go, ga
+        return e.value, (shells_to_atoms(go, self.orb_centers, atom_xyz)
+                         + shells_to_atoms(ga, self.aux_centers, atom_xyz))
+
     # -- parity entry points --------------------------------------------
     def eri3c_dense(self):
         t = self.torch
@@ -271,7 +317,11 @@ class Plan:
 class DFSpec:
     """Density-fitting spec (``dftax/ks/terms.py:63-76``) with the B200 backend.
 
-    ``chunk`` must be ``None`` (materialized): the library holds B in HBM.
+    ``chunk=None`` or ``"auto"``: B is built once and held in device memory
+    (dftax's materialized ``DFCoulomb``). An integer ``chunk`` selects the
+    streamed form (``StreamedDFCoulomb``, ``terms.py:716-761``): B is not
+    stored and every J/K evaluation rebuilds it chunk by chunk of bra pairs
+    (the chunk size is the library's own: the value only selects the form).
     """
 
     auxbasis: object = None
@@ -287,14 +337,14 @@ def df(auxbasis=None, *, chunk=None, screen=None, spherical=None, backend="b200"
     """``dftax.df`` (``terms.py:96-148``) plus ``backend``/``precision``."""
     if backend != "b200":
         raise ValueError("this package provides only backend='b200'")
-    if chunk not in (None, "auto"):
-        raise ValueError("the b200 backend materializes B; chunk must be None or 'auto'")
+    if chunk not in (None, "auto") and not (isinstance(chunk, int) and chunk > 0):
+        raise ValueError("chunk must be None, 'auto' or a positive int (streamed)")
     if spherical is False:
         raise ValueError("the b200 backend fits in the spherical auxiliary span")
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
-    return DFSpec(auxbasis=auxbasis, chunk=None, screen=screen, spherical=spherical,
-                  backend=backend, precision=precision)
+    return DFSpec(auxbasis=auxbasis, chunk=chunk if isinstance(chunk, int) else None,
+                  screen=screen, spherical=spherical, backend=backend, precision=precision)
 
 
 class CoulombTerm(abc.ABC):
@@ -317,13 +367,14 @@ class B200DFCoulomb(CoulombTerm):
 
     def __init__(self, basis: BasisData, aux_basis: BasisData, hf_coeff: float, *,
                  hf_coeff_lr: float = 0.0, omega: float = 0.0, screen: float | None = None,
-                 precision: str = "fp64", device: int = 0):
+                 precision: str = "fp64", streamed: bool = False, device: int = 0):
         if hf_coeff_lr != 0.0 and omega <= 0.0:
             raise ValueError("hf_coeff_lr needs omega > 0 (terms.py:953-978)")
         self.hf_coeff = float(hf_coeff)
         self.hf_coeff_lr = float(hf_coeff_lr)
         self.plan = Plan(basis, aux_basis, screen=screen, precision=precision,
-                         omega=omega if hf_coeff_lr != 0.0 else 0.0, device=device)
+                         omega=omega if hf_coeff_lr != 0.0 else 0.0, streamed=streamed,
+                         device=device)
         self.plan.build()
 
     def energy(self, P, S=None, nocc=None) -> float:
@@ -337,6 +388,14 @@ class B200DFCoulomb(CoulombTerm):
     def jk(self, C, w=None):
         return self.plan.jk(C, w)
 
+    def geometry_gradient(self, P, atom_xyz):
+        """dE/dR (natom, 3) of this term at the fixed density P: the part of
+        dftax's forces() that flows through the DF integral build
+        (``forces.py:245-270``). Long-range exchange is not included."""
+        if self.hf_coeff_lr != 0.0:
+            raise NotImplementedError("geometry gradient of the long-range exchange")
+        return self.plan.energy_grad(P, self.hf_coeff, atom_xyz)[1]
+
 
 def make_coulomb(spec: DFSpec, basis: BasisData, hf_coeff: float, *, hf_coeff_lr: float = 0.0,
                  omega: float = 0.0, device: int = 0):
@@ -346,7 +405,8 @@ def make_coulomb(spec: DFSpec, basis: BasisData, hf_coeff: float, *, hf_coeff_lr
     if not isinstance(spec.auxbasis, BasisData):
         raise TypeError("spec.auxbasis must be a built BasisData")
     return B200DFCoulomb(basis, spec.auxbasis, hf_coeff, hf_coeff_lr=hf_coeff_lr, omega=omega,
-                         screen=spec.screen, precision=spec.precision, device=device)
+                         screen=spec.screen, precision=spec.precision,
+                         streamed=spec.chunk is not None, device=device)
 
 
 __all__ = ["Context", "Plan", "DFSpec", "df", "CoulombTerm", "B200DFCoulomb", "make_coulomb"]

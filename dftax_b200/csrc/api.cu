@@ -11,6 +11,7 @@
 #include <mutex>
 #include <numeric>
 #include <exception>
+#include <functional>
 #include <thread>
 
 namespace dfjk {
@@ -691,7 +692,7 @@ void check_finite(Plan& p, const double* x, int64_t n, cudaStream_t s, const cha
   if (h) fail(DFJK_ERR_NUMERIC, "non-finite values in %s", what);
 }
 
-static int64_t chunk_budget(const Plan& p) {
+int64_t chunk_budget(const Plan& p) {
   return p.opts.chunk_bytes > 0 ? p.opts.chunk_bytes : (int64_t)2 << 30;
 }
 
@@ -737,7 +738,7 @@ void compute_metric_factor(Plan& p, cudaStream_t s) {
 }
 
 // Pair chunks of at most `budget` bytes of raw rows (ld doubles each).
-static std::vector<std::pair<int64_t, int64_t>> pair_chunks(const Plan& p, int64_t ld, int64_t budget) {
+std::vector<std::pair<int64_t, int64_t>> pair_chunks(const Plan& p, int64_t ld, int64_t budget) {
   std::vector<std::pair<int64_t, int64_t>> out;
   const int64_t npair = (int64_t)p.pair_s1.size();
   const int64_t max_rows = std::max<int64_t>(budget / (ld * (int64_t)sizeof(double)), 49);
@@ -755,7 +756,7 @@ static std::vector<std::pair<int64_t, int64_t>> pair_chunks(const Plan& p, int64
   return out;
 }
 
-static int64_t rows_of(const Plan& p, int64_t b, int64_t e) {
+int64_t rows_of(const Plan& p, int64_t b, int64_t e) {
   const int64_t npair = (int64_t)p.pair_s1.size();
   const int64_t end_row = e < npair ? p.pair_row0[e] : p.nrows;
   return end_row - p.pair_row0[b];
@@ -782,7 +783,6 @@ void build(Plan& p, cudaStream_t s) {
   p.timer.mark(kPhPairs, s);
   launch_pair_setup(p, s);
   p.timer.mark(kPhPairs, s);
-  p.d_B.ensure((size_t)std::max<int64_t>(p.nrows, 1) * p.ldb * sizeof(double));
   const bool mixed = p.opts.precision == DFJK_MIXED;
   const int64_t ld = p.naux;
   const int64_t kp = (p.naux + 15) / 16 * 16;
@@ -797,6 +797,15 @@ void build(Plan& p, cudaStream_t s) {
   ozaki_prepare_l(p, s);
   p.ws_oz_raw.ensure((size_t)build_digits(p) * maxrows * kp);
   p.ws_oz_er.ensure((size_t)maxrows * sizeof(int));
+  if (p.opts.streamed) {
+    // B is rebuilt chunk by chunk by every J/K call (for_each_b_chunk)
+    p.d_B.free();
+    p.ws_bchunk.ensure((size_t)maxrows * p.ldb * sizeof(double));
+    ozaki_check(p, s);
+    p.built = 1;
+    return;
+  }
+  p.d_B.ensure((size_t)std::max<int64_t>(p.nrows, 1) * p.ldb * sizeof(double));
   for (auto& ch : chunks) {
     const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
     p.timer.mark(kPhEri3c, s);
@@ -820,6 +829,22 @@ void build(Plan& p, cudaStream_t s) {
     p.timer.mark(kPhKplanes, s);
   }
   p.built = 1;
+}
+
+void for_each_b_chunk(Plan& p, cudaStream_t s,
+                      const std::function<void(int64_t r0, int64_t nr, const double* Bc)>& fn) {
+  const int64_t kp = (p.naux + 15) / 16 * 16;
+  auto chunks = pair_chunks(p, p.naux, chunk_budget(p));
+  for (auto& ch : chunks) {
+    const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
+    launch_eri3c_rows(p, ch.first, ch.second, r0, p.ws_raw.p, p.naux, false, s);
+    ozaki_split_raw(p, p.ws_raw.as<double>(), nr, p.ws_oz_raw.as<int8_t>(), nr * kp,
+                    p.ws_oz_er.as<int>(), s);
+    ozaki_bgemm(p, p.ws_oz_raw.as<int8_t>(), nr * kp, p.ws_oz_er.as<int>(), nr,
+                p.ws_bchunk.as<double>(), s);
+    fn(r0, nr, p.ws_bchunk.as<double>());
+  }
+  ozaki_check(p, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -985,6 +1010,8 @@ dfjk_status dfjk_plan_create(dfjk_ctx* h, const dfjk_basis* orb, const dfjk_basi
       fail(DFJK_ERR_INVALID, "unknown precision %d", pl->p.opts.precision);
     if (!(pl->p.opts.omega >= 0.0) || !std::isfinite(pl->p.opts.omega))
       fail(DFJK_ERR_INVALID, "omega must be finite and >= 0");
+    if (pl->p.opts.streamed != 0 && pl->p.opts.streamed != 1)
+      fail(DFJK_ERR_INVALID, "streamed must be 0 or 1");
     make_plan(pl->p, orb, aux);
     if (pl->p.opts.omega > 0.0) {
       // the long-range operator over the same bases; its Schwarz screen is the
@@ -1129,6 +1156,21 @@ dfjk_status dfjk_energy_rsh(dfjk_plan* pl, const double* P, int32_t nspin, doubl
   });
 }
 
+dfjk_status dfjk_energy_grad(dfjk_plan* pl, const double* P, int32_t nspin, double hf_coeff,
+                             double* e, double* grad_orb, double* grad_aux, void* stream) {
+  if (!pl) return DFJK_ERR_INVALID;
+  return guard(pl->p.ctx, [&] {
+    if (!pl->p.built) fail(DFJK_ERR_STATE, "dfjk_energy_grad before dfjk_build");
+    if (pl->p.opts.streamed)
+      fail(DFJK_ERR_UNSUPPORTED, "dfjk_energy_grad needs B held in device memory (not streamed)");
+    if (!P || !e || !grad_orb || !grad_aux || (nspin != 1 && nspin != 2))
+      fail(DFJK_ERR_INVALID, "bad gradient arguments");
+    if (!std::isfinite(hf_coeff)) fail(DFJK_ERR_INVALID, "non-finite exchange coefficient");
+    DFJK_CUDA(cudaSetDevice(pl->p.ctx->device));
+    *e = energy_gradient(pl->p, P, nspin, hf_coeff, grad_orb, grad_aux, st(stream));
+  });
+}
+
 dfjk_status dfjk_eri3c_dense(dfjk_plan* pl, double* out, void* stream) {
   if (!pl || !out) return DFJK_ERR_INVALID;
   return guard(pl->p.ctx, [&] {
@@ -1183,6 +1225,16 @@ dfjk_status dfjk_boys(dfjk_ctx* h, const double* t, int64_t n, int32_t nmax, dou
     if (!t || !out || n < 0 || nmax < 0 || nmax > 18) fail(DFJK_ERR_INVALID, "bad boys arguments");
     DFJK_CUDA(cudaSetDevice(h->c.device));
     launch_boys(h->c, t, n, nmax, out, st(stream));
+  });
+}
+
+dfjk_status dfjk_wait_selftest(dfjk_ctx* h, int64_t limit_ns, double* waited_ms, void* stream) {
+  if (!h) return DFJK_ERR_INVALID;
+  return guard(&h->c, [&] {
+    if (limit_ns < 1000 || limit_ns > 4000000000ll)
+      fail(DFJK_ERR_INVALID, "wait limit %lld ns outside [1e3, 4e9]", (long long)limit_ns);
+    DFJK_CUDA(cudaSetDevice(h->c.device));
+    wait_selftest(h->c, limit_ns, waited_ms, st(stream));
   });
 }
 

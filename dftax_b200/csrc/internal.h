@@ -3,6 +3,8 @@
 
 #include "common.h"
 
+#include <functional>
+
 namespace dfjk {
 
 struct Plan;
@@ -91,6 +93,8 @@ struct Plan {
   PhaseTimer timer;
   // persistent workspaces (grow-only), reused by every build and J/K call
   DevBuf ws_raw, ws_syevd, ws_info, ws_flag, ws_dvec, ws_gamma, ws_part, ws_X, ws_Cp, ws_sel;
+  // streamed plans: one chunk of B rows, the chunk's K-list bounds
+  DevBuf ws_bchunk, ws_kb, ws_ke;
   // mixed precision: int8 digit planes of the square B_x for the tensor-core half transform
   DevBuf d_oz_a, d_oz_ea;
   int64_t nao_p16 = 0, naux_p16 = 0;
@@ -118,6 +122,17 @@ void ozaki_k1(Plan& p, int64_t nsel, int64_t x0, int64_t n, double* X, cudaStrea
 void ozaki_syrk(Plan& p, const double* X, int64_t kt, double sign, bool beta0, double* K,
                 cudaStream_t s);
 
+// ---- 3-center row chunks (api.cu) ----
+int64_t chunk_budget(const Plan& p);   // bytes of one chunk of 3-center rows
+// runs [first, end) of kept pairs whose rows x ld doubles fit in budget bytes
+std::vector<std::pair<int64_t, int64_t>> pair_chunks(const Plan& p, int64_t ld, int64_t budget);
+int64_t rows_of(const Plan& p, int64_t b, int64_t e);   // rows of pairs [b, e)
+// Streamed plans: rebuilds B chunk by chunk of kept pairs (the build's
+// kernels) and calls fn(first row, rows, chunk) for each, in row order; the
+// chunk (rows x ldb) is valid during the call on stream s.
+void for_each_b_chunk(Plan& p, cudaStream_t s,
+                      const std::function<void(int64_t r0, int64_t nr, const double* Bc)>& fn);
+
 // ---- kernels & launchers (md.cu) ----
 void boys_table_host(std::vector<double>& tbl, std::vector<double>& asym);
 void launch_boys(const Context& c, const double* t, int64_t n, int nmax, double* out, cudaStream_t s);
@@ -131,7 +146,14 @@ void launch_schwarz(const Context& c, Shells& sh, const std::vector<int>& pa,
 // ---- contractions (jk.cu) ----
 void jk_compute(Plan& p, const double* C, const double* w, int64_t ncol, double* J, double* K,
                 cudaStream_t s);
-double j_energy_from_density(Plan& p, const double* Ptot, double* J, cudaStream_t s);
+// gamma = B^T vec(Ptot) over the plan's rows (ldb doubles; the J intermediate)
+void gamma_from_density(Plan& p, const double* Ptot, double* gamma, cudaStream_t s);
+
+// ---- nuclear gradient of the DF energy (grad.cu) ----
+// E and dE/dR at a fixed density P (nspin x nao x nao, device): per orbital
+// shell and per auxiliary shell (device, [n][3], overwritten)
+double energy_gradient(Plan& p, const double* P, int nspin, double hf, double* grad_orb,
+                       double* grad_aux, cudaStream_t s);
 
 void check_finite(Plan& p, const double* x, int64_t n, cudaStream_t s, const char* what);
 

@@ -129,8 +129,44 @@ static int num_sms(int dev) {
   return n > 0 ? n : 148;
 }
 
+__global__ void add_to_kernel(const double* __restrict__ x, int64_t n, double* __restrict__ y) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
+}
+
+// gamma (+)= Bc^T dvec over nrows rows of Bc: fixed-order partial sums
+static void gamma_rows(Plan& p, const double* Bc, int64_t nrows, const double* dvec, double* out,
+                       bool add, cudaStream_t s) {
+  const int sms = num_sms(p.ctx->device);
+  const int64_t ycols = (p.ldb + kGtCols - 1) / kGtCols;
+  int64_t xparts = std::max<int64_t>(1, (int64_t)sms * 4 / ycols);
+  xparts = std::min<int64_t>(xparts, std::max<int64_t>(1, nrows));
+  const int64_t rows_per = (nrows + xparts - 1) / xparts;
+  xparts = (nrows + rows_per - 1) / rows_per;
+  DevBuf& part = p.ws_part;
+  part.ensure((size_t)(std::max<int64_t>(xparts, 1) + (add ? 1 : 0)) * p.ldb * sizeof(double));
+  double* sum = part.as<double>() + xparts * p.ldb;   // the chunk's gamma when adding
+  gamma_partial_kernel<<<dim3((unsigned)xparts, (unsigned)ycols), kGtThreads, 0, s>>>(
+      Bc, p.ldb, nrows, dvec, rows_per, part.as<double>());
+  DFJK_LAUNCHED();
+  reduce_rows_kernel<<<(unsigned)((p.ldb + 255) / 256), 256, 0, s>>>(part.as<double>(), xparts,
+                                                                     p.ldb, add ? sum : out);
+  DFJK_LAUNCHED();
+  if (add) {
+    add_to_kernel<<<(unsigned)((p.ldb + 255) / 256), 256, 0, s>>>(sum, p.ldb, out);
+    DFJK_LAUNCHED();
+  }
+}
+
 // gamma = B^T dvec into `gamma` (ldb doubles)
 static void gamma_from_dvec(Plan& p, const double* dvec, double* gamma, cudaStream_t s) {
+  if (p.opts.streamed) {
+    DFJK_CUDA(cudaMemsetAsync(gamma, 0, p.ldb * sizeof(double), s));
+    for_each_b_chunk(p, s, [&](int64_t r0, int64_t nr, const double* Bc) {
+      if (nr > 0) gamma_rows(p, Bc, nr, dvec + r0, gamma, true, s);
+    });
+    return;
+  }
   const int sms = num_sms(p.ctx->device);
   const int64_t ycols = (p.ldb + kGtCols - 1) / kGtCols;
   int64_t xparts = std::max<int64_t>(1, (int64_t)sms * 4 / ycols);
@@ -155,6 +191,17 @@ static void j_from_gamma(Plan& p, const double* gamma, double* J, cudaStream_t s
   DFJK_CUDA(cudaMemsetAsync(J, 0, (size_t)p.nao * p.nao * sizeof(double), s));
   if (p.nrows == 0) return;
   const int sms = num_sms(p.ctx->device);
+  if (p.opts.streamed) {
+    for_each_b_chunk(p, s, [&](int64_t r0, int64_t nr, const double* Bc) {
+      if (nr == 0) return;
+      const int64_t warps = std::min<int64_t>(nr, (int64_t)sms * 64);
+      j_rows_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
+          Bc, p.ldb, nr, gamma, p.d_row_m.as<int>() + r0, p.d_row_n.as<int>() + r0,
+          p.d_row_w.as<int8_t>() + r0, p.nao, J);
+      DFJK_LAUNCHED();
+    });
+    return;
+  }
   const int64_t warps = std::min<int64_t>(p.nrows, (int64_t)sms * 64);
   j_rows_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
       p.d_B.as<double>(), p.ldb, p.nrows, gamma, p.d_row_m.as<int>(), p.d_row_n.as<int>(),
@@ -187,10 +234,14 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool val
                : "memory");
 }
 
+// The list of m is entries [kbeg[m], kend[m]) (kend == nullptr: up to
+// kbeg[m + 1]); entry e reads B row krow[e] - row0. accumulate: X += instead
+// of X = (a streamed plan sums the chunks of B rows).
 __global__ void __launch_bounds__(256) half_transform_kernel(
     const double* __restrict__ B, int64_t ldb, int64_t x0, int64_t xc, const double* __restrict__ Cp,
-    int64_t ncol, const int* __restrict__ kptr, const int* __restrict__ krow,
-    const int* __restrict__ kn, double* __restrict__ X) {
+    int64_t ncol, const int* __restrict__ kbeg, const int* __restrict__ kend,
+    const int* __restrict__ krow, const int* __restrict__ kn, int64_t row0, int accumulate,
+    double* __restrict__ X) {
   // two buffers: chunk c + 1 is copied (cp.async) while chunk c is multiplied
   __shared__ double Bs[2][kHtK][kHtPX];
   __shared__ double Cs[2][kHtK][kHtPI];
@@ -205,13 +256,13 @@ __global__ void __launch_bounds__(256) half_transform_kernel(
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 5; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-  const int e0 = kptr[m], e1 = kptr[m + 1];
+  const int e0 = kbeg[m], e1 = kend ? kend[m] : kbeg[m + 1];
   // kHtK list entries: rows of B (x tile) and rows of C' (i tile)
   auto stage = [&](int buf, int e) {
     for (int q = threadIdx.x; q < kHtK * kHtX; q += 256) {
       const int k = q / kHtX, x = q % kHtX;
       const bool ok = e + k < e1 && xt + x < xc;
-      cp_async8(&Bs[buf][k][x], ok ? B + (int64_t)krow[e + k] * ldb + x0 + xt + x : B, ok);
+      cp_async8(&Bs[buf][k][x], ok ? B + ((int64_t)krow[e + k] - row0) * ldb + x0 + xt + x : B, ok);
     }
     for (int q = threadIdx.x; q < kHtK * kHtI; q += 256) {
       const int k = q / kHtI, i = q % kHtI;
@@ -254,9 +305,32 @@ __global__ void __launch_bounds__(256) half_transform_kernel(
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         const int64_t i = it + wi + 8 * b + 2 * fk + r;
-        if (i < ncol) X[((int64_t)m * xc + x) * ncol + i] = acc[a][b][r];
+        if (i < ncol) {
+          double* o = X + ((int64_t)m * xc + x) * ncol + i;
+          *o = accumulate ? *o + acc[a][b][r] : acc[a][b][r];
+        }
       }
   }
+}
+
+// [kb[m], ke[m]): the entries of m's K list whose rows lie in [r0, r1) (each
+// list is in ascending row order)
+__global__ void list_bounds_kernel(const int* __restrict__ kptr, const int* __restrict__ krow,
+                                   int64_t nao, int64_t r0, int64_t r1, int* __restrict__ kb,
+                                   int* __restrict__ ke) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m >= nao) return;
+  auto lower = [&](int lo, int hi, int64_t v) {
+    while (lo < hi) {
+      const int mid = lo + (hi - lo) / 2;
+      if (krow[mid] < v) lo = mid + 1;
+      else hi = mid;
+    }
+    return lo;
+  };
+  const int lo = kptr[m], hi = kptr[m + 1];
+  kb[m] = lower(lo, hi, r0);
+  ke[m] = lower(lo, hi, r1);
 }
 
 // K partials on the float64 tensor cores: for the lower-triangle tile pair
@@ -410,8 +484,15 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
                                                                          dsel.as<int>(), nsel,
                                                                          Cp.as<double>());
   DFJK_LAUNCHED();
-  // x chunking so that X (nao * xc * nsel doubles) stays within budget
-  const int64_t budget = (int64_t)6 << 30;
+  // x chunking so that X (nao * xc * nsel doubles) stays within budget; a
+  // streamed plan rebuilds B once per x chunk, so it takes up to half the
+  // free device memory
+  int64_t budget = (int64_t)6 << 30;
+  if (p.opts.streamed) {
+    size_t fr = 0, tot = 0;
+    DFJK_CUDA(cudaMemGetInfo(&fr, &tot));
+    budget = std::max<int64_t>(budget, (int64_t)(fr / 2));
+  }
   int64_t xc = budget / (nao * nsel * (int64_t)sizeof(double));
   xc = std::max<int64_t>(kHtX, xc / kHtX * kHtX);
   xc = std::min<int64_t>(xc, (p.nfit + kHtX - 1) / kHtX * kHtX);
@@ -423,18 +504,36 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
     const int64_t n = std::min(xc, p.nfit - x0);
     dim3 grid((unsigned)nao, (unsigned)((n + kHtX - 1) / kHtX), (unsigned)((nsel + kHtI - 1) / kHtI));
     p.timer.mark(kPhKhalf, s);
-    if (p.opts.precision == DFJK_MIXED) {
+    const bool oz = p.opts.precision == DFJK_MIXED && !p.opts.streamed;
+    if (p.opts.streamed) {
+      // X = sum over chunks of B rows of the half transform of each chunk
+      DFJK_CUDA(cudaMemsetAsync(X.p, 0, (size_t)nao * n * nsel * sizeof(double), s));
+      p.ws_kb.ensure(nao * sizeof(int));
+      p.ws_ke.ensure(nao * sizeof(int));
+      for_each_b_chunk(p, s, [&](int64_t r0, int64_t nr, const double* Bc) {
+        list_bounds_kernel<<<(unsigned)((nao + 255) / 256), 256, 0, s>>>(
+            p.d_kptr.as<int>(), p.d_krow.as<int>(), nao, r0, r0 + nr, p.ws_kb.as<int>(),
+            p.ws_ke.as<int>());
+        DFJK_LAUNCHED();
+        half_transform_kernel<<<grid, 256, 0, s>>>(Bc, p.ldb, x0, n, Cp.as<double>(), nsel,
+                                                   p.ws_kb.as<int>(), p.ws_ke.as<int>(),
+                                                   p.d_krow.as<int>(), p.d_kn.as<int>(), r0, 1,
+                                                   X.as<double>());
+        DFJK_LAUNCHED();
+      });
+    } else if (oz) {
       if (x0 == 0) ozaki_prepare_c(p, Cp.as<double>(), nsel, s);
       ozaki_k1(p, nsel, x0, n, X.as<double>(), s);   // int8 tensor cores, exact accumulation
     } else {
       half_transform_kernel<<<grid, 256, 0, s>>>(p.d_B.as<double>(), p.ldb, x0, n, Cp.as<double>(),
-                                                 nsel, p.d_kptr.as<int>(), p.d_krow.as<int>(),
-                                                 p.d_kn.as<int>(), X.as<double>());
+                                                 nsel, p.d_kptr.as<int>(), nullptr,
+                                                 p.d_krow.as<int>(), p.d_kn.as<int>(), 0, 0,
+                                                 X.as<double>());
       DFJK_LAUNCHED();
     }
     p.timer.mark(kPhKhalf, s);
     p.timer.mark(kPhKsyrk, s);
-    if (p.opts.precision == DFJK_MIXED) {
+    if (oz) {
       ozaki_syrk(p, X.as<double>(), n * nsel, sign, beta0, K, s);   // full square, int8 tensor cores
     } else {
       syrk_fp64(p, X.as<double>(), n * nsel, sign, beta0, K, s);
@@ -576,6 +675,18 @@ static void density_factor(Plan& p, const double* Q, DevBuf& Ct, DevBuf& dw, cud
 
 // hf_lr: the long-range exchange of range-separated hybrids through the plan's
 // long-range fit (terms.py:604-612)
+void gamma_from_density(Plan& p, const double* Ptot, double* gamma, cudaStream_t s) {
+  DevBuf dvec;
+  dvec.alloc(std::max<int64_t>(p.nrows, 1) * sizeof(double));
+  if (p.nrows > 0) {
+    dvec_from_density_kernel<<<(unsigned)((p.nrows + 255) / 256), 256, 0, s>>>(
+        Ptot, p.nao, p.d_row_m.as<int>(), p.d_row_n.as<int>(), p.d_row_w.as<int8_t>(), p.nrows,
+        dvec.as<double>());
+    DFJK_LAUNCHED();
+  }
+  gamma_from_dvec(p, dvec.as<double>(), gamma, s);
+}
+
 double energy(Plan& p, const double* P, int nspin, double hf, double hf_lr, double* F,
               cudaStream_t s) {
   const int64_t n = p.nao, nn = n * n;

@@ -174,6 +174,8 @@ extern "C" dfjk_status dfjk_j_noalloc(dfjk_plan* pl, const double* C, const doub
     if (!C || !J || ncol <= 0) dfjk::fail(DFJK_ERR_INVALID, "C or J is null or ncol=%lld", (long long)ncol);
     if (pl->p.opts.precision != DFJK_FP64)
       dfjk::fail(DFJK_ERR_UNSUPPORTED, "dfjk_j_noalloc needs a float64 plan");
+    if (pl->p.opts.streamed)
+      dfjk::fail(DFJK_ERR_UNSUPPORTED, "dfjk_j_noalloc needs B held in device memory (not streamed)");
     DFJK_CUDA(cudaSetDevice(c->device));
     dfjk::j_noalloc(pl->p, C, w, ncol, J, static_cast<cudaStream_t>(stream));
   });

@@ -75,4 +75,11 @@ void ozaki_map_out(CUtensorMap* m, double* base, int64_t cols, int64_t batches, 
 void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, int grid_z,
                   cudaStream_t s);
 
+// The bounded wait of the tensor-core pipelines, made to run out: one block
+// waits limit_ns on a barrier nothing completes (a second warp with the
+// pipelines' own 4 s limit returns when the first one's timeout is flagged);
+// fails with the pipelines' timeout error. waited_ms[0..1]: each warp's wait.
+constexpr int kWaitSelftestCode = 90;
+void wait_selftest(const Context& c, int64_t limit_ns, double* waited_ms, cudaStream_t s);
+
 }  // namespace dfjk

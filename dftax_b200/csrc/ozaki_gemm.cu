@@ -63,13 +63,14 @@ __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, int* err, int code) {
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, int* err, int code,
+                                          unsigned long long limit_ns = kWaitNs) {
   if (mbar_try(addr, parity)) return true;
   const uint64_t t0 = now_ns();
   while (true) {
     if (mbar_try(addr, parity)) return true;
     if (*reinterpret_cast<volatile int*>(err) != 0) return false;
-    if (now_ns() - t0 > kWaitNs) {
+    if (now_ns() - t0 > limit_ns) {
       atomicCAS(err, 0, code);
       return false;
     }
@@ -787,6 +788,50 @@ void ozaki_launch(OzakiShape shape, const OzakiMaps& maps, const OzakiArgs& a, i
     case kOzSyrk: launch<5, 64, 96, 3, false>(maps, a, grid_z, s); return;
   }
   fail(DFJK_ERR_INVALID, "unknown int8 GEMM shape %d", (int)shape);
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded wait
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Warp 0 waits on an mbarrier that no thread arrives at, with the given limit;
+// warp 1 waits on it with the pipelines' own limit and must return as soon as
+// warp 0's timeout is flagged. Nothing else is in flight, so the block only
+// has to return.
+__global__ void wait_selftest_kernel(int* err, unsigned long long limit_ns,
+                                     unsigned long long* waited) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t a = smem_u32(&bar);
+  if (threadIdx.x == 0) mbar_init(a, 1);
+  __syncthreads();
+  const int warp = threadIdx.x / 32;
+  const uint64_t t0 = now_ns();
+  mbar_wait(a, 0, err, kWaitSelftestCode + warp, warp == 0 ? limit_ns : kWaitNs);
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) waited[warp] = now_ns() - t0;
+}
+
+}  // namespace
+
+void wait_selftest(const Context& c, int64_t limit_ns, double* waited_ms, cudaStream_t s) {
+  (void)c;
+  DevBuf buf;
+  buf.alloc(32);
+  DFJK_CUDA(cudaMemsetAsync(buf.p, 0, 32, s));
+  int* err = buf.as<int>();
+  auto* waited = reinterpret_cast<unsigned long long*>(buf.as<char>() + 16);
+  wait_selftest_kernel<<<1, 64, 0, s>>>(err, (unsigned long long)limit_ns, waited);
+  DFJK_LAUNCHED();
+  int h = 0;
+  unsigned long long w[2] = {0, 0};
+  DFJK_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaMemcpyAsync(w, waited, sizeof(w), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  if (waited_ms)
+    for (int i = 0; i < 2; ++i) waited_ms[i] = 1e-6 * (double)w[i];
+  if (h) fail(DFJK_ERR_CUDA, "tensor-core pipeline gave up waiting (code %d)", h);
 }
 
 }  // namespace dfjk

@@ -76,7 +76,8 @@ class KS:
         self.nocc = (nelec // 2,)
         self.xc = xc
         self.plan = plan or Plan(basis, coulomb.auxbasis, screen=coulomb.screen,
-                                 precision=coulomb.precision, device=device)
+                                 precision=coulomb.precision,
+                                 streamed=coulomb.chunk is not None, device=device)
         if not self.plan.info()["built"]:
             self.plan.build()
         self.ctx, self.lib, self.dev = self.plan.ctx, self.plan.lib, self.plan.dev

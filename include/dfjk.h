@@ -66,7 +66,11 @@ typedef struct {
                            (dftax df(screen=...), eri3c_bucketed.py:140-169)     */
   double metric_cutoff; /* relative metric eigenvalue cutoff (terms.py:191)     */
   int32_t precision;    /* DFJK_FP64 or DFJK_MIXED                               */
-  int32_t reserved;
+  int32_t streamed;     /* 0: B is built once and held in device memory; 1: B is
+                           not stored: every J/K call rebuilds it chunk by chunk
+                           of bra pairs (dftax's StreamedDFCoulomb, terms.py:716-
+                           761), for systems whose B exceeds device memory. K
+                           then runs the float64 half transform on each chunk */
   int64_t chunk_bytes;  /* staging budget for raw 3-center rows (0 = default)   */
   double omega;         /* > 0: also build the long-range erf(omega r)/r fit for
                            range-separated exchange (energy.py:419-433); 0: off */
@@ -154,6 +158,19 @@ dfjk_status dfjk_energy(dfjk_plan* plan, const double* P, int32_t nspin, double 
 dfjk_status dfjk_energy_rsh(dfjk_plan* plan, const double* P, int32_t nspin, double hf_coeff,
                             double hf_coeff_lr, double* e, double* F, void* stream);
 
+/* Nuclear gradient of the DF energy at a fixed symmetric density P
+ * [nspin][nao][nao] (device): the geometry derivative dftax's forces() take
+ * through the integral build (forces.py:245-270), with the metric
+ * pseudo-inverse differentiated by d(V+) = -V+ dV V+ (terms.py:196-204).
+ * Writes dE/d(center) of every orbital shell, grad_orb [norb_shell][3], and
+ * of every auxiliary shell, grad_aux [naux_shell][3] (device, shell order of
+ * the bases given to dfjk_plan_create; an atom's gradient is the sum over
+ * the shells on it), and the energy -> *e (host). hf_coeff as in
+ * dfjk_energy; plans with omega > 0 (attenuated operator) give the gradient
+ * of their own operator's energy. Host-synchronizing. */
+dfjk_status dfjk_energy_grad(dfjk_plan* plan, const double* P, int32_t nspin, double hf_coeff,
+                             double* e, double* grad_orb, double* grad_aux, void* stream);
+
 /* J of D = C diag(w) C^T, as dfjk_jk computes it, without allocating any
  * device memory: for callers that must not call cudaMalloc while they run
  * (an XLA FFI handler inside a JAX program whose allocator already owns the
@@ -212,6 +229,15 @@ dfjk_status dfjk_kept_pairs(const dfjk_plan* plan, int32_t* out);
  * (dftax/energy/boys.py:130-176); nmax <= 18. */
 dfjk_status dfjk_boys(dfjk_ctx* ctx, const double* t, int64_t n, int32_t nmax, double* out,
                       void* stream);
+
+/* Runs the bounded wait of the tensor-core pipelines (an mbarrier wait that
+ * gives up after a %globaltimer limit and flags the error) on a barrier that
+ * nothing completes: one warp with a limit of limit_ns (1e3 .. 4e9), a second
+ * with the pipelines' own 4 s limit, which must return as soon as the first
+ * one's timeout is flagged. Returns DFJK_ERR_CUDA with the pipelines'
+ * timeout message; waited_ms[0..1] (host, optional) receive each warp's wait.
+ * Nothing else is in flight in the block, and the context stays usable. */
+dfjk_status dfjk_wait_selftest(dfjk_ctx* ctx, int64_t limit_ns, double* waited_ms, void* stream);
 
 #ifdef __cplusplus
 }

@@ -191,4 +191,90 @@ def df_build_jk(orb, aux, C, hf_coeff: float = 0.25, nthreads: int | None = None
     return {"J": J, "K": K, "E": float(E), "seconds": t}
 
 
-__all__ = ["build_lib", "eri3c_dense", "eri2c", "df_build_jk", "k_reference_path", "threads"]
+
+
+# ---------------------------------------------------------------------------
+# Nuclear gradient of the DF energy at a fixed density
+# ---------------------------------------------------------------------------
+
+def _moved(basis, atom_xyz, atom: int, axis: int, h: float):
+    """A copy of ``basis`` whose functions on ``atom`` are moved by h along axis."""
+    import dataclasses
+
+    cen = np.array(basis.centers, dtype=np.float64, copy=True)
+    on = np.linalg.norm(cen - np.asarray(atom_xyz)[atom], axis=1) < 1e-8
+    cen[on, axis] += h
+    return dataclasses.replace(basis, centers=cen)
+
+
+def df_energy_terms(orb, aux, P, hf_coeff: float, nthreads: int | None = None, vinv=None):
+    """The DF energy of ``DFCoulomb.energy`` (``terms.py:592-613``) at a fixed
+    density P (nspin, nao, nao) and the two weights its geometry derivative
+    contracts with the integral derivatives:
+
+        dE = sum_{mnP} G[m,n,P] d(mn|P) - 1/2 sum_{PQ} W[P,Q] d(P|Q)
+
+    with gamma = V+ c, c_P = sum P_tot (mn|P), and for each spin channel s of
+    exchange weight k_s (-a_x/4 closed shell, -a_x/2 per spin):
+    G = gamma_P P_tot + sum_s 2 k_s P_s Z_P P_s, Z_P = sum_Q V+_PQ (..|Q), and
+    W = gamma gamma^T + sum_s 2 k_s V+ M_s V+, M_s[P,Q] = tr(P_s T_P P_s T_Q).
+    The metric enters through d(V+) = -V+ dV V+, the rule of dftax's
+    ``_metric_pinv_jvp`` (``terms.py:196-204``). ``vinv`` replaces the
+    oracle's own pseudo-inverse (to separate the conditioning of the metric
+    from the rest when comparing)."""
+    P = np.asarray(P, dtype=np.float64)
+    if P.ndim == 2:
+        P = P[None]
+    if vinv is None:
+        vinv = odf.metric_pinv(eri2c(aux, nthreads))
+    I3 = eri3c_dense(orb, aux, nthreads=nthreads)
+    nao, _, naux = I3.shape
+    Ptot = P.sum(0)
+    c = np.einsum("mn,mnP->P", Ptot, I3)
+    gam = vinv @ c
+    E = 0.5 * c @ gam
+    G = Ptot[:, :, None] * gam[None, None, :]
+    W = np.outer(gam, gam)
+    ks = [-0.25 * hf_coeff] if P.shape[0] == 1 else [-0.5 * hf_coeff] * P.shape[0]
+    if hf_coeff != 0.0:
+        Z = (I3.reshape(nao * nao, naux) @ vinv).reshape(nao, nao, naux)
+        for Ps, k in zip(P, ks):
+            Y = np.einsum("ml,lsP,sn->mnP", Ps, I3, Ps, optimize=True)
+            M = np.einsum("mnP,nmQ->PQ", Y, I3, optimize=True)
+            E += k * np.einsum("PQ,PQ->", vinv, M)
+            G += 2.0 * k * np.einsum("ml,lsP,sn->mnP", Ps, Z, Ps, optimize=True)
+            W += 2.0 * k * (vinv @ M @ vinv)
+    return float(E), G, W
+
+
+def df_energy_grad(orb, aux, P, hf_coeff: float, atom_xyz, h: float = 1e-3,
+                   nthreads: int | None = None, vinv=None):
+    """dE/dR (natom, 3) of the DF energy at fixed P: G and W from
+    ``df_energy_terms`` contracted with the derivatives of (mn|P) and (P|Q)
+    with respect to each atom's position (the functions on the atom move
+    together), taken by central differences at h and h/2 with one Richardson
+    step (error O(h^4)). Returns (E, grad)."""
+    E, G, W = df_energy_terms(orb, aux, P, hf_coeff, nthreads, vinv)
+    atom_xyz = np.asarray(atom_xyz, dtype=np.float64)
+
+    def phi(atom, axis, d):
+        o, a = _moved(orb, atom_xyz, atom, axis, d), _moved(aux, atom_xyz, atom, axis, d)
+        return (np.einsum("mnP,mnP->", G, eri3c_dense(o, a, nthreads=nthreads))
+                - 0.5 * np.einsum("PQ,PQ->", W, eri2c(a, nthreads)))
+
+    grad = np.zeros((len(atom_xyz), 3))
+    for A in range(len(atom_xyz)):
+        for x in range(3):
+            d1 = (phi(A, x, h) - phi(A, x, -h)) / (2 * h)
+            d2 = (phi(A, x, h / 2) - phi(A, x, -h / 2)) / h
+            grad[A, x] = (4.0 * d2 - d1) / 3.0
+    return E, grad
+
+
+def df_energy(orb, aux, P, hf_coeff: float, nthreads: int | None = None) -> float:
+    """The DF energy alone (``df_energy_terms``'s first value)."""
+    return df_energy_terms(orb, aux, P, hf_coeff, nthreads)[0]
+
+
+__all__ = ["build_lib", "eri3c_dense", "eri2c", "df_build_jk", "k_reference_path", "threads",
+           "df_energy_terms", "df_energy_grad", "df_energy"]

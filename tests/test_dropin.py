@@ -28,11 +28,13 @@ def test_df_spec_defaults_and_fields():
                                                                           "mixed", None)
     assert df().precision == "fp64"
     assert df(chunk="auto").chunk is None   # "auto" resolves to materialized B
+    assert df(chunk=4096).chunk == 4096     # an integer chunk selects the streamed form
 
 
 @pytest.mark.parametrize("kw,msg", [
     ({"backend": "jax"}, "backend"),
-    ({"chunk": 4096}, "chunk"),
+    ({"chunk": -1}, "chunk"),
+    ({"chunk": "big"}, "chunk"),
     ({"spherical": False}, "spherical"),
     ({"precision": "bf16"}, "precision"),
 ])

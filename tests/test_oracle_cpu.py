@@ -83,3 +83,32 @@ def test_k_path_equals_einsum(cpu):
     D = rng.standard_normal((7, 7))
     D = D + D.T
     assert rel(cpu.k_reference_path(I3, vinv, D), odf.df_k(I3, vinv, D)) < 1e-13
+
+
+@pytest.mark.parametrize("nspin", [1, 2])
+def test_gradient_oracle_equals_finite_differences(cpu, nspin):
+    """The oracle's DF gradient (weights G, W contracted with integral
+    derivatives) against central differences of the whole oracle energy, on
+    the water molecule with its own orbital basis as the fitting basis: that
+    metric is well conditioned and drops no direction, so the pseudo-inverse
+    rule d(V+) = -V+ dV V+ is the exact derivative and both must agree."""
+    from dftax_b200 import systems
+
+    _, xyz, orb, _, nocc = systems.workload("water", seed=0)
+    aux = orb
+    C = systems.random_occupied(orb.nao, nocc, seed=1)
+    P = 2.0 * C @ C.T if nspin == 1 else np.stack([C @ C.T, C[:, :-1] @ C[:, :-1].T])
+    E, g = cpu.df_energy_grad(orb, aux, P, 0.25, xyz)
+    assert abs(E - cpu.df_energy(orb, aux, P, 0.25)) < 1e-12 * abs(E)
+    h = 1e-3
+    fd = np.zeros_like(g)
+    for A in range(len(xyz)):
+        for x in range(3):
+            def e(d):
+                return cpu.df_energy(cpu._moved(orb, xyz, A, x, d), cpu._moved(aux, xyz, A, x, d),
+                                     P, 0.25)
+            d1 = (e(h) - e(-h)) / (2 * h)
+            d2 = (e(h / 2) - e(-h / 2)) / h
+            fd[A, x] = (4 * d2 - d1) / 3
+    assert np.abs(fd - g).max() < 1e-7 * np.abs(g).max()
+    assert np.abs(g.sum(axis=0)).max() < 1e-9 * np.abs(g).max()
