@@ -82,13 +82,21 @@ void* cache_take(int dev, size_t n, size_t* got) {
 }
 }  // namespace
 
+std::recursive_mutex& capture_mutex() {
+  static std::recursive_mutex m;
+  return m;
+}
+
 void sync_device(int dev) {
   uint64_t s0;
   {
     std::lock_guard<std::mutex> lk(g_cache_mu);
     s0 = free_seq()[dev];
   }
-  DFJK_CUDA(cudaDeviceSynchronize());
+  {
+    std::lock_guard<std::recursive_mutex> cap(capture_mutex());
+    DFJK_CUDA(cudaDeviceSynchronize());
+  }
   std::lock_guard<std::mutex> lk(g_cache_mu);
   idle_upto()[dev] = std::max(idle_upto()[dev], s0);
 }
@@ -103,6 +111,7 @@ void cache_trim(int dev) {
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(dev);
+  std::lock_guard<std::recursive_mutex> cap(capture_mutex());
   for (auto& c : v) cudaFree(c.p);
   cudaSetDevice(cur);
 }
@@ -985,7 +994,10 @@ dfjk_status dfjk_destroy(dfjk_ctx* h) {
   if (h->c.cublas) cublasDestroy(h->c.cublas);
   if (h->c.cusolver) cusolverDnDestroy(h->c.cusolver);
   const int dev = h->c.device;
-  cudaDeviceSynchronize();
+  {
+    std::lock_guard<std::recursive_mutex> cap(dfjk::capture_mutex());
+    cudaDeviceSynchronize();
+  }
   delete h;
   dfjk::cache_trim(dev);
   return DFJK_OK;
@@ -1058,7 +1070,10 @@ dfjk_status dfjk_plan_destroy(dfjk_plan* pl) {
 dfjk_status dfjk_trim(dfjk_ctx* h) {
   if (!h) return DFJK_ERR_INVALID;
   cudaSetDevice(h->c.device);
-  cudaDeviceSynchronize();
+  {
+    std::lock_guard<std::recursive_mutex> cap(dfjk::capture_mutex());
+    cudaDeviceSynchronize();
+  }
   dfjk::cache_trim(h->c.device);
   return DFJK_OK;
 }

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <exception>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -75,6 +76,11 @@ struct Error {
 // synchronization began is idle (may be handed out again without waiting).
 void sync_device(int dev);
 void cache_trim(int dev);            // cudaFree every cached buffer of dev
+// Held while a stream of this library captures a CUDA graph, and by every
+// device-wide synchronization (cudaDeviceSynchronize, cudaFree) the library
+// makes: those fail while any stream of the device is capturing, and the
+// batch engine's workers capture and allocate from different threads.
+std::recursive_mutex& capture_mutex();
 
 // Device buffer owned by a plan or context (allocated through the cache).
 struct DevBuf {

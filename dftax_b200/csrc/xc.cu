@@ -644,15 +644,20 @@ double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, co
     if (!ws.cap) DFJK_CUDA(cudaStreamCreateWithFlags(&ws.cap, cudaStreamNonBlocking));
     const int64_t k0 = dfjk_kernel_launches();
     cudaGraph_t graph = nullptr;
-    bool ok = cudaStreamBeginCapture(ws.cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    if (ok) {
-      try {
-        xc_enqueue(c, ov, pts, w, P, Vxc, xp, ws, ws.cap);
-      } catch (...) {
-        ok = false;
+    bool ok;
+    {
+      // no other thread of the library synchronizes the device meanwhile
+      std::lock_guard<std::recursive_mutex> cap(capture_mutex());
+      ok = cudaStreamBeginCapture(ws.cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        try {
+          xc_enqueue(c, ov, pts, w, P, Vxc, xp, ws, ws.cap);
+        } catch (...) {
+          ok = false;
+        }
+        const cudaError_t ec = cudaStreamEndCapture(ws.cap, &graph);
+        ok = ok && ec == cudaSuccess && graph;
       }
-      const cudaError_t ec = cudaStreamEndCapture(ws.cap, &graph);
-      ok = ok && ec == cudaSuccess && graph;
     }
     if (ok) ok = cudaGraphInstantiate(&ws.exec, graph, 0) == cudaSuccess;
     if (graph) cudaGraphDestroy(graph);
