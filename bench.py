@@ -67,6 +67,8 @@ def parse():
                     help="also solve a batch of this many water clusters (64: the 64-cluster "
                          "batch, n log-uniform in [3, 40])")
     ap.add_argument("--workers", type=int, default=4, help="concurrent solves of the engine")
+    ap.add_argument("--guess", default="sad", choices=["sad", "core"],
+                    help="SCF starting density of the SCF, serving and batch measurements")
     ap.add_argument("--screen", type=float, default=0.0,
                     help="relative Schwarz screen of shell pairs (0: none, the default)")
     return ap.parse_args()
@@ -493,8 +495,10 @@ def scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks):
     """SCF solves/s of the workload from geometry, per precision: the DF plan
     and build, the Becke grid (75 radial shells, 302-point Lebedev, NWChem
     pruning), one-electron integrals and the DIIS iterations of a closed-shell
-    DF-PBE0 SCF from the core-Hamiltonian guess, to |dE| < 1e-8 Ha and a
-    commutator below 1e-6 (dftax's defaults). One untimed solve first."""
+    DF-PBE0 SCF from the --guess density (``sad``: superposition of atomic
+    densities, the per-element atomic solves cached by the untimed first
+    solve, their assembly timed; ``core``: the core Hamiltonian), to
+    |dE| < 1e-8 Ha and a commutator below 1e-6 (dftax's defaults)."""
     from dftax_b200 import df
     from dftax_b200.ks import KS, scf
 
@@ -503,7 +507,7 @@ def scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks):
     for prec in precs:
         def solve():
             ks = KS(sym, xyz, orb, coulomb=df(aux, precision=prec))
-            r = scf(ks)
+            r = scf(ks, guess=args.guess)
             ks.close()
             ks.plan.close()
             return r
@@ -526,9 +530,10 @@ def scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks):
     head = precs[0]
     line = dict(out[head])
     line["precision"] = head
+    line["guess"] = args.guess
     line["what"] = ("one closed-shell DF-PBE0 SCF from geometry: plan and DF build, Becke grid "
-                    "(75 x 302, NWChem pruning), one-electron integrals, core guess, DIIS to "
-                    "|dE| < 1e-8 Ha and commutator < 1e-6")
+                    f"(75 x 302, NWChem pruning), one-electron integrals, {args.guess} guess, "
+                    "DIIS to |dE| < 1e-8 Ha and commutator < 1e-6")
     if "fp64" in out and head != "fp64":
         line["fp64"] = out["fp64"]
         line["speedup_vs_fp64"] = round(out["fp64"]["ms_per_solve"] / out[head]["ms_per_solve"], 3)
@@ -540,8 +545,9 @@ def _loguniform_ints(rng, lo, hi, n):
     return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), n))).astype(int)
 
 
-def _requests(eng, mols, grids, prec):
-    return [eng.request(s, x, o, a, grid=g, precision=prec) for (s, x, o, a), g in zip(mols, grids)]
+def _requests(eng, mols, grids, prec, guess=None):
+    return [eng.request(s, x, o, a, grid=g, precision=prec, guess=guess)
+            for (s, x, o, a), g in zip(mols, grids)]
 
 
 def serve_measure(args, precs, rank):
@@ -573,7 +579,7 @@ def serve_measure(args, precs, rank):
     out, energies, ok_mask = {}, {}, {}
     for prec in precs:
         with BatchEngine(workers=args.workers) as eng:
-            reqs = _requests(eng, mols, grids, prec)
+            reqs = _requests(eng, mols, grids, prec, args.guess)
             # one untimed pass, all at once: the XC chunk autotuner settles its
             # per-size choices and the device-memory cache fills, as in a
             # server that has been running
@@ -607,6 +613,7 @@ def serve_measure(args, precs, rank):
     line["stream"] = {"requests": n, "rate_per_s": args.serve_rate, "workers": args.workers,
                       "water_n": [3, args.serve_max_water], "alkane_n": [4, args.serve_max_alkane],
                       "molecules": names, "seed": 50 + rank,
+                      "guess": args.guess,
                       "what": "closed-shell DF-PBE0 SCF per request, Becke 75 x 302 grid"}
     if "fp64" in out and head != "fp64":
         line["fp64"] = out["fp64"]
@@ -636,7 +643,8 @@ def batch_measure(args, precs, rank):
     for prec in precs:
         with BatchEngine(workers=args.workers) as eng:
             t0 = time.perf_counter()
-            ids = [eng.submit(*m, grid=g, precision=prec) for m, g in zip(mols, grids)]
+            ids = [eng.submit(*m, grid=g, precision=prec, guess=args.guess)
+                   for m, g in zip(mols, grids)]
             res = [eng.wait(i) for i in ids]
             sec = time.perf_counter() - t0
         energies[prec] = np.array([r.e_tot for r in res])
@@ -650,7 +658,7 @@ def batch_measure(args, precs, rank):
     line = dict(out[head])
     line["precision"] = head
     line["clusters"] = {"count": int(args.batch), "n": ns.tolist(), "seed": 64 + rank,
-                        "workers": args.workers}
+                        "workers": args.workers, "guess": args.guess}
     if "fp64" in out and head != "fp64":
         line["fp64"] = out["fp64"]
         d = np.abs(energies[head] - energies["fp64"])

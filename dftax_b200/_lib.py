@@ -98,7 +98,8 @@ class BatchRequest(ctypes.Structure):
     _fields_ = [("orb", POINTER(Basis)), ("aux", POINTER(Basis)), ("plan_opts", Options),
                 ("natom", c_int32), ("nocc", c_int32), ("atom_xyz", c_void_p),
                 ("atom_charge", c_void_p), ("npoint", c_int64), ("grid_xyz", c_void_p),
-                ("grid_w", c_void_p), ("scf_opts", ScfOptions), ("P_out", c_void_p)]
+                ("grid_w", c_void_p), ("scf_opts", ScfOptions), ("P_out", c_void_p),
+                ("P_guess", c_void_p)]
 
 
 class BatchResult(ctypes.Structure):

@@ -21,6 +21,7 @@ from . import _lib
 from .basis import BasisData
 from .coulomb import PRECISIONS, _basis_struct
 from .grid import ATOMIC_NUMBER, Becke, becke_grid
+from .guess import initial_density
 from .ks import XC_FUNCTIONALS
 
 
@@ -120,9 +121,11 @@ class BatchEngine:
 
 
 def make_request(symbols, coords_bohr, orb: BasisData, aux: BasisData, *, xc="PBE0",
-                 precision="fp64", grid=None, screen=None, scf_opts=None):
+                 precision="fp64", grid=None, screen=None, scf_opts=None, guess=None):
     """A dfbatch_request for an explicit grid (points, weights) and the arrays
-    it points into (kept alive by the caller until it is submitted)."""
+    it points into (kept alive by the caller until it is submitted).
+    ``guess``: None/``"core"`` (core Hamiltonian), ``"sad"`` (superposition of
+    atomic densities, built here) or an explicit (nao, nao) density."""
     lib = _lib.load()
     coords = np.ascontiguousarray(np.asarray(coords_bohr, dtype=np.float64).reshape(-1, 3))
     charges = np.ascontiguousarray([float(ATOMIC_NUMBER[s]) for s in symbols])
@@ -152,14 +155,19 @@ def make_request(symbols, coords_bohr, orb: BasisData, aux: BasisData, *, xc="PB
     r.scf_opts.hf_coeff, r.scf_opts.x_scale, r.scf_opts.c_scale = hf, xs, cs
     for k, v in (scf_opts or {}).items():
         setattr(r.scf_opts, k, v)
+    P0 = initial_density(guess, list(symbols), coords, orb, aux, nelec)
+    if P0 is not None:
+        P0 = np.ascontiguousarray(P0, dtype=np.float64).reshape(orb.nao, orb.nao)
+        keep.append(P0)
+        r.P_guess = P0.ctypes.data
     return r, keep, orb.nao
 
 
 def scf_batch(molecules, *, precision="fp64", xc="PBE0", grid=None, workers: int = 4,
-              hbm_budget: int = 0, device: int = 0, want_density=False):
+              hbm_budget: int = 0, device: int = 0, want_density=False, guess=None):
     """Solve every (symbols, coords, orb, aux) of ``molecules``; results in order."""
     with BatchEngine(device, workers, hbm_budget) as eng:
-        ids = [eng.submit(s, x, o, a, precision=precision, xc=xc, grid=grid,
+        ids = [eng.submit(s, x, o, a, precision=precision, xc=xc, grid=grid, guess=guess,
                           want_density=want_density) for (s, x, o, a) in molecules]
         return [eng.wait(i) for i in ids]
 

@@ -58,6 +58,7 @@ struct Job {
   int64_t npoint = 0;
   std::vector<double> xyz, charge, gxyz, gw;
   double* P_out = nullptr;
+  std::vector<double> P0;   // initial density (empty: core guess)
   int64_t bytes = 0;
   dfbatch_result res{};
   bool done = false;
@@ -147,7 +148,13 @@ void run_job(dfjk_ctx* ctx, cudaStream_t s, Job& j) {
     check(dfscf_create(plan, j.natom, j.xyz.data(), j.charge.data(), j.npoint,
                        j.npoint ? j.gxyz.data() : nullptr, j.npoint ? j.gw.data() : nullptr, j.nocc,
                        &j.sopts, &scf, s));
-    check(dfscf_run(scf, nullptr, nullptr, s));
+    dfjk::DevBuf P0;
+    if (!j.P0.empty()) {
+      P0.alloc(j.P0.size() * sizeof(double));
+      DFJK_CUDA(cudaMemcpyAsync(P0.p, j.P0.data(), j.P0.size() * sizeof(double),
+                                cudaMemcpyHostToDevice, s));
+    }
+    check(dfscf_run(scf, j.P0.empty() ? nullptr : P0.as<double>(), nullptr, s));
     check(dfscf_get_result(scf, &j.res.scf));
     if (j.P_out) {
       dfjk_plan_info info;
@@ -297,6 +304,10 @@ dfjk_status dfbatch_submit(dfbatch* e, const dfbatch_request* r, int64_t* id) {
       j->gw.assign(r->grid_w, r->grid_w + r->npoint);
     }
     j->P_out = r->P_out;
+    if (r->P_guess) {
+      const int64_t nao = r->orb->cart2sph ? r->orb->nsph : r->orb->ncart;
+      j->P0.assign(r->P_guess, r->P_guess + nao * nao);
+    }
     j->bytes = estimate(r);
     if (j->bytes > e->budget)
       fail(DFJK_ERR_MEMORY, "request needs about %lld bytes, above the budget of %lld",

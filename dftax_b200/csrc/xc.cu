@@ -205,11 +205,12 @@ __global__ void scatter_v_kernel(const double* __restrict__ Vc, int nsig, const 
   V[(int64_t)map[b] * nao + map[a]] += Vc[i];
 }
 
-// rho[g] = sum_mu X Phi, grad[x][g] = 2 sum_mu X dPhi_x. A block takes 32
-// points with 8 lanes of mu each (mu = lane, lane + 8, ...: a warp reads 32
-// consecutive points of one mu), and the 8 partial sums are added in a fixed
-// order, so the result does not depend on the launch.
-constexpr int kRhoPts = 32, kRhoLanes = 8;
+// rho[g] = sum_mu X Phi, grad[x][g] = 2 sum_mu X dPhi_x. A block takes 16
+// points with 16 lanes of mu each (mu = lane, lane + 16, ...: a warp reads 16
+// consecutive points of two mu rows), so an 8192-point chunk fills 512
+// blocks; the 16 partial sums are added in a fixed order, so the result does
+// not depend on the launch.
+constexpr int kRhoPts = 16, kRhoLanes = 16;
 __global__ void __launch_bounds__(kRhoPts * kRhoLanes) rho_kernel(
     const double* __restrict__ X, const double* __restrict__ phi, const double* __restrict__ dphi,
     int nao, int64_t G, int64_t ng, double* __restrict__ rho, double* __restrict__ grad) {

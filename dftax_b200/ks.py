@@ -9,8 +9,9 @@ quadrature grid and the canonical orthonormalizer, all on the device
 
 Functionals: ``"PBE0"`` (0.75 PBE exchange + PBE correlation + 0.25 exact
 exchange, ``xc.py:584-601``), ``"PBE"`` and ``"HF"`` (exact exchange only, no
-grid). The guess is the core Hamiltonian (``guess.core()``) or an explicit
-density; dftax's minao/SAD guesses are not provided.
+grid). The guess is the core Hamiltonian (``guess.core()``, the default),
+a superposition of atomic densities (``guess.sad()`` or ``"sad"``) or an
+explicit density; dftax's minao guess is not provided.
 """
 
 from __future__ import annotations
@@ -25,6 +26,7 @@ from . import _lib
 from .basis import BasisData
 from .coulomb import DFSpec, Plan, _stream_ptr, _torch
 from .grid import ATOMIC_NUMBER, Becke, becke_grid
+from .guess import CoreSpec, SADSpec, initial_density
 
 XC_FUNCTIONALS = {
     # name: (hf_coeff, x_scale, c_scale)
@@ -75,6 +77,7 @@ class KS:
             raise NotImplementedError("this SCF is closed-shell: an even electron count is needed")
         self.nocc = (nelec // 2,)
         self.xc = xc
+        self.basis, self.aux = basis, coulomb.auxbasis
         self.plan = plan or Plan(basis, coulomb.auxbasis, screen=coulomb.screen,
                                  precision=coulomb.precision,
                                  streamed=coulomb.chunk is not None, device=device)
@@ -183,6 +186,9 @@ def scf(ks: KS, *, max_iter: int = 128, e_tol: float = 1e-8, d_tol: float = 1e-6
     o.max_iter, o.e_tol, o.d_tol, o.level_shift = int(max_iter), float(e_tol), float(d_tol), \
         float(level_shift)
     P0 = None
+    if isinstance(guess, (str, SADSpec, CoreSpec)):
+        guess = initial_density(guess, ks.symbols, ks.coords, ks.basis, ks.aux,
+                                2 * ks.nocc[0], ks.ctx.device)
     if guess is not None:
         P0 = ks._dev(guess)
         if P0.ndim == 3:
@@ -227,17 +233,19 @@ def _main(argv=None):
     ap.add_argument("--radial", type=int, default=75)
     ap.add_argument("--lebedev", type=int, default=302)
     ap.add_argument("--repeat", type=int, default=1, help="solves (the last one is reported)")
+    ap.add_argument("--guess", default="core", choices=["core", "sad"])
     a = ap.parse_args(argv)
     sym, xyz, orb, aux, nocc = systems.workload(a.workload, seed=0)
     for _ in range(a.repeat):
         t0 = time.perf_counter()
         ks = KS(sym, xyz, orb, coulomb=df(aux, precision=a.precision), xc=a.xc,
                 grid=becke(a.radial, a.lebedev))
-        r = scf(ks)
+        r = scf(ks, guess=a.guess)
         sec = time.perf_counter() - t0
         ks.close()
         ks.plan.close()
     print(json.dumps({"workload": a.workload, "precision": a.precision, "xc": a.xc,
+                      "guess": a.guess,
                       "e_tot": r.e_tot, "converged": r.converged, "n_iter": r.n_iter,
                       "seconds": round(sec, 3), "parts_ms": r.timings_ms,
                       "xc_chunk": r.xc_chunk, "xc_graph": r.xc_graph}))

@@ -51,6 +51,10 @@ typedef struct {
   const double* grid_w;
   dfscf_options scf_opts;
   double* P_out;                /* optional host [nao][nao]: the converged density      */
+  const double* P_guess;        /* optional host [nao][nao] initial density (a
+                                   superposition of atomic densities, guess.py:529-546,
+                                   or a previous solve's); NULL: the core-Hamiltonian
+                                   guess                                                */
 } dfbatch_request;
 
 typedef struct {

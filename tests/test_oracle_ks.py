@@ -127,3 +127,30 @@ def test_scf_converges_to_a_stationary_density(scf_golden, orb, water_golden):
     # aufbau: the occupied orbitals lie below the virtual ones (the synthetic
     # even-tempered basis has no tight O 1s exponents, so E is about -60 Ha)
     assert eps[4] < 0.0 < eps[5] or eps[4] < eps[5]
+
+
+def test_ground_state_configurations():
+    """Madelung filling with the s -> d promotions of Cr, Cu and the 4d row."""
+    from dftax_b200.guess import ground_state
+
+    assert ground_state(1) == [(1, 0, 1)]
+    assert ground_state(8) == [(1, 0, 2), (2, 0, 2), (2, 1, 4)]
+    assert dict(((n, l), c) for n, l, c in ground_state(24))[(3, 2)] == 5
+    assert dict(((n, l), c) for n, l, c in ground_state(29))[(4, 0)] == 1
+    assert (5, 0) not in dict(((n, l), c) for n, l, c in ground_state(46))
+    for Z in range(1, 55):
+        assert sum(c for _, _, c in ground_state(Z)) == Z
+
+
+def test_config_occupations_fill_channels_by_energy():
+    """A synthetic spherical atom: orbitals of pure l, the lowest s pair and
+    the p triplet of oxygen's 1s2 2s2 2p4."""
+    import numpy as np
+
+    from dftax_b200.guess import config_occupations
+
+    ao_l = [0, 0, 0, 1, 1, 1]
+    S = np.eye(6)
+    C = np.eye(6)[:, [0, 3, 4, 5, 1, 2]]   # energy order: s, p, p, p, s, s
+    occ = config_occupations(C, S, ao_l, 8)
+    assert np.allclose(occ, [2, 4 / 3, 4 / 3, 4 / 3, 2, 0])
