@@ -14,10 +14,13 @@
 //   as the double-where of grid.py:31-44 makes them);
 //   W = v_rho/2 Phi + v_grad . dPhi, V += Phi^T W               (cuBLAS DGEMM);
 // and at the end Vxc = V + V^T, the symmetrized P-gradient of E_xc
-// (scf.py:42-46). The energy is summed per block in a fixed order and then
-// over blocks on the host, so it is reproducible. The SCF calls this with
+// (scf.py:42-46). The chunks run on kXcBranches concurrent streams (chunk k
+// on branch k % kXcBranches, one V accumulator each, summed in branch order
+// at the end); the energy is summed per block in a fixed order and then over
+// blocks on the host, so the result is reproducible. The SCF calls this with
 // the same buffers every iteration: the second call captures its launches
-// (about eight per chunk) in a CUDA graph and later calls replay it.
+// (about eight per chunk, the branches forked and joined by events) in a
+// CUDA graph and later calls replay it.
 #include "md_device.cuh"
 #include "scf.h"
 
@@ -72,12 +75,6 @@ __global__ void becke_kernel(const double* __restrict__ pts, const int* __restri
 // ---------------------------------------------------------------------------
 // AO values and gradients
 // ---------------------------------------------------------------------------
-
-__device__ __forceinline__ double ipow(double x, int n) {
-  double r = 1.0;
-  for (int k = 0; k < n; ++k) r *= x;
-  return r;
-}
 
 // p[n] for 0 <= n <= L (p[0] for n < 0) by selects, so p stays in registers
 // whether or not n folds to a constant
@@ -399,11 +396,17 @@ __global__ void w_kernel(const double* __restrict__ phi, const double* __restric
   W[i] = v;
 }
 
-__global__ void symmetrize_add_kernel(const double* __restrict__ V, int n, double* __restrict__ out) {
+// out = sum over the nb branch accumulators V_b (n x n, stride n*n) of
+// V_b + V_b^T, in branch order
+__global__ void symmetrize_sum_kernel(const double* __restrict__ V, int nb, int n,
+                                      double* __restrict__ out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= (int64_t)n * n) return;
+  const int64_t nn = (int64_t)n * n;
+  if (i >= nn) return;
   const int64_t r = i / n, c = i % n;
-  out[i] = V[i] + V[c * n + r];
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += V[b * nn + i] + V[b * nn + c * n + r];
+  out[i] = s;
 }
 
 }  // namespace
@@ -461,16 +464,31 @@ void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
   double lo[3] = {INFINITY, INFINITY, INFINITY};
   for (int64_t i = 0; i < n; ++i)
     for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], pts[3 * i + d]);
-  std::vector<std::pair<uint64_t, int64_t>> key(n);
+  std::vector<uint64_t> code(n);
+  uint64_t cmax = 0;
   for (int64_t i = 0; i < n; ++i) {
     uint64_t c[3];
     for (int d = 0; d < 3; ++d) c[d] = (uint64_t)std::floor(pts[3 * i + d] - lo[d]);
-    key[i] = {morton3(c[0], c[1], c[2]), i};
+    code[i] = morton3(c[0], c[1], c[2]);
+    cmax = std::max(cmax, code[i]);
   }
-  std::sort(key.begin(), key.end());
+  // order by (code, index): a stable counting sort over the codes when they
+  // are few (a molecule spans a few dozen cells per axis), else a sort
+  std::vector<int64_t> order(n);
+  if (cmax < ((uint64_t)1 << 24)) {
+    std::vector<int64_t> start(cmax + 2, 0);
+    for (int64_t i = 0; i < n; ++i) start[code[i] + 1]++;
+    for (uint64_t k = 0; k <= cmax; ++k) start[k + 1] += start[k];
+    for (int64_t i = 0; i < n; ++i) order[start[code[i]]++] = i;
+  } else {
+    std::vector<std::pair<uint64_t, int64_t>> key(n);
+    for (int64_t i = 0; i < n; ++i) key[i] = {code[i], i};
+    std::sort(key.begin(), key.end());
+    for (int64_t i = 0; i < n; ++i) order[i] = key[i].second;
+  }
   std::vector<double> p2(3 * n), w2(n);
   for (int64_t i = 0; i < n; ++i) {
-    const int64_t j = key[i].second;
+    const int64_t j = order[i];
     for (int d = 0; d < 3; ++d) p2[3 * i + d] = pts[3 * j + d];
     w2[i] = w[j];
   }
@@ -553,60 +571,76 @@ void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>&
 static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, const double* w,
                        const double* P, double* Vxc, const XcParams& xp, XcWork& ws,
                        cudaStream_t s) {
+  (void)c;
   const int nao = ov.nao;
+  const int64_t nn = (int64_t)nao * nao;
   const XcChunks& ch = ws.ch;
   const int64_t G = ch.G;
   const int64_t nchunk = (int64_t)ch.g0.size();
   const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
-  DFJK_CUBLAS(cublasSetStream(c.cublas, s));
-  if (Vxc) DFJK_CUDA(cudaMemsetAsync(ws.Vacc.p, 0, (size_t)nao * nao * sizeof(double), s));
   const double one = 1.0, zero = 0.0;
+  // fork: every branch starts after the caller's prior work on s
+  DFJK_CUDA(cudaEventRecord(ws.fork, s));
+  for (XcBranch& b : ws.br) {
+    DFJK_CUDA(cudaStreamWaitEvent(b.s, ws.fork, 0));
+    DFJK_CUBLAS(cublasSetStream(b.blas, b.s));
+  }
+  if (Vxc)
+    for (int q = 0; q < kXcBranches; ++q)
+      DFJK_CUDA(cudaMemsetAsync(ws.Vacc.as<double>() + q * nn, 0, nn * sizeof(double), ws.br[q].s));
   for (int64_t k = 0; k < nchunk; ++k) {
+    XcBranch& b = ws.br[k % kXcBranches];
+    cudaStream_t bs = b.s;
+    double* Vacc = ws.Vacc.as<double>() + (k % kXcBranches) * nn;
     const int64_t g0 = ch.g0[k], ng = ch.ng[k];
     const int nsig = ch.ao_cnt[k], nsh = ch.sh_cnt[k];
     const int* map = ch.d_ao_map.as<int>() + ch.ao_off[k];
     if (nsig == 0) {
-      DFJK_CUDA(cudaMemsetAsync(ws.ered.as<double>() + k * nblk, 0, nblk * sizeof(double), s));
+      DFJK_CUDA(cudaMemsetAsync(ws.ered.as<double>() + k * nblk, 0, nblk * sizeof(double), bs));
       continue;
     }
     const int64_t plane = (int64_t)nsig * G;
     ao_kernel<<<dim3((unsigned)((G + kAoThreads - 1) / kAoThreads), (unsigned)nsh), kAoThreads, 0,
-                s>>>(ov, ch.d_sh.as<int>() + ch.sh_off[k], ch.d_sh_out0.as<int>() + ch.sh_off[k],
-                     pts, g0, ng, G, nsig, ws.phi.as<double>(), ws.dphi.as<double>());
+                bs>>>(ov, ch.d_sh.as<int>() + ch.sh_off[k], ch.d_sh_out0.as<int>() + ch.sh_off[k],
+                      pts, g0, ng, G, nsig, b.phi.as<double>(), b.dphi.as<double>());
     DFJK_LAUNCHED();
-    gather_p_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, s>>>(
-        P, nao, map, nsig, ws.Pc.as<double>());
+    gather_p_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, bs>>>(
+        P, nao, map, nsig, b.Pc.as<double>());
     DFJK_LAUNCHED();
     // X (G x nsig, column-major: [k][g]) = Phi Pc
-    DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nsig, nsig, &one,
-                            ws.phi.as<double>(), (int)G, ws.Pc.as<double>(), nsig, &zero,
-                            ws.X.as<double>(), (int)G));
-    rho_kernel<<<(unsigned)((ng + kRhoPts - 1) / kRhoPts), kRhoPts * kRhoLanes, 0, s>>>(
-        ws.X.as<double>(), ws.phi.as<double>(), ws.dphi.as<double>(), nsig, G, ng,
-        ws.vr.as<double>(), ws.vg.as<double>());
+    DFJK_CUBLAS(cublasDgemm(b.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nsig, nsig, &one,
+                            b.phi.as<double>(), (int)G, b.Pc.as<double>(), nsig, &zero,
+                            b.X.as<double>(), (int)G));
+    rho_kernel<<<(unsigned)((ng + kRhoPts - 1) / kRhoPts), kRhoPts * kRhoLanes, 0, bs>>>(
+        b.X.as<double>(), b.phi.as<double>(), b.dphi.as<double>(), nsig, G, ng,
+        b.vr.as<double>(), b.vg.as<double>());
     DFJK_LAUNCHED();
-    pbe_kernel<<<(unsigned)nblk, kPtThreads, 0, s>>>(ws.vr.as<double>(), ws.vg.as<double>(),
-                                                     w + g0, G, ng, xp.x_scale, xp.c_scale,
-                                                     xp.rho_thresh, ws.ered.as<double>() + k * nblk);
+    pbe_kernel<<<(unsigned)nblk, kPtThreads, 0, bs>>>(b.vr.as<double>(), b.vg.as<double>(),
+                                                      w + g0, G, ng, xp.x_scale, xp.c_scale,
+                                                      xp.rho_thresh, ws.ered.as<double>() + k * nblk);
     DFJK_LAUNCHED();
     if (Vxc) {
-      w_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(
-          ws.phi.as<double>(), ws.dphi.as<double>(), ws.vr.as<double>(), ws.vg.as<double>(), nsig,
-          G, ng, ws.W.as<double>());
+      w_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, bs>>>(
+          b.phi.as<double>(), b.dphi.as<double>(), b.vr.as<double>(), b.vg.as<double>(), nsig,
+          G, ng, b.W.as<double>());
       DFJK_LAUNCHED();
-      // Vc = Phi^T W, scattered into V
-      DFJK_CUBLAS(cublasDgemm(c.cublas, CUBLAS_OP_T, CUBLAS_OP_N, nsig, nsig, (int)G, &one,
-                              ws.phi.as<double>(), (int)G, ws.W.as<double>(), (int)G, &zero,
-                              ws.Vc.as<double>(), nsig));
-      scatter_v_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, s>>>(
-          ws.Vc.as<double>(), nsig, map, nao, ws.Vacc.as<double>());
+      // Vc = Phi^T W, scattered into this branch's V
+      DFJK_CUBLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, nsig, nsig, (int)G, &one,
+                              b.phi.as<double>(), (int)G, b.W.as<double>(), (int)G, &zero,
+                              b.Vc.as<double>(), nsig));
+      scatter_v_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, bs>>>(
+          b.Vc.as<double>(), nsig, map, nao, Vacc);
       DFJK_LAUNCHED();
     }
   }
+  // join: s waits for every branch
+  for (XcBranch& b : ws.br) {
+    DFJK_CUDA(cudaEventRecord(b.done, b.s));
+    DFJK_CUDA(cudaStreamWaitEvent(s, b.done, 0));
+  }
   if (Vxc) {
-    const int64_t n2 = (int64_t)nao * nao;
-    symmetrize_add_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(ws.Vacc.as<double>(), nao,
-                                                                        Vxc);
+    symmetrize_sum_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(ws.Vacc.as<double>(),
+                                                                        kXcBranches, nao, Vxc);
     DFJK_LAUNCHED();
   }
 }
@@ -620,16 +654,24 @@ double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, co
   const int64_t nchunk = (int64_t)ch.g0.size();
   const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
   const int64_t plane_max = (int64_t)std::max(ch.max_ao, 1) * G;
-  ws.phi.ensure(plane_max * sizeof(double));
-  ws.dphi.ensure(3 * plane_max * sizeof(double));
-  ws.X.ensure(plane_max * sizeof(double));
-  ws.W.ensure(plane_max * sizeof(double));
-  ws.Pc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
-  ws.Vc.ensure((size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double));
-  ws.vr.ensure(G * sizeof(double));
-  ws.vg.ensure(3 * G * sizeof(double));
+  const size_t sq = (size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double);
+  for (XcBranch& b : ws.br) {
+    b.phi.ensure(plane_max * sizeof(double));
+    b.dphi.ensure(3 * plane_max * sizeof(double));
+    b.X.ensure(plane_max * sizeof(double));
+    b.W.ensure(plane_max * sizeof(double));
+    b.Pc.ensure(sq);
+    b.Vc.ensure(sq);
+    b.vr.ensure(G * sizeof(double));
+    b.vg.ensure(3 * G * sizeof(double));
+    // streams, events and handles are made here, never during a capture
+    if (!b.s) DFJK_CUDA(cudaStreamCreateWithFlags(&b.s, cudaStreamNonBlocking));
+    if (!b.done) DFJK_CUDA(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+    if (!b.blas) DFJK_CUBLAS(cublasCreate(&b.blas));
+  }
+  if (!ws.fork) DFJK_CUDA(cudaEventCreateWithFlags(&ws.fork, cudaEventDisableTiming));
   ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
-  if (Vxc) ws.Vacc.ensure((size_t)nao * nao * sizeof(double));
+  if (Vxc) ws.Vacc.ensure((size_t)kXcBranches * nao * nao * sizeof(double));
   const void* args[4] = {P, Vxc, pts, w};
   const bool same = std::equal(args, args + 4, ws.g_args);
   if (ws.exec && same) {
