@@ -11,6 +11,7 @@
 // solve made alone runs, with the same fixed-order reductions, so a result
 // does not depend on what else is running.
 #include "internal.h"
+#include "scf.h"
 #include "../../include/dfbatch.h"
 
 #include <chrono>
@@ -112,9 +113,9 @@ int64_t estimate(const dfbatch_request* r) {
   const int64_t diis = r->scf_opts.diis_space > 0 ? r->scf_opts.diis_space : 8;
   b += (14 + 2 * diis) * nao * nao * 8;                          // SCF matrices, DIIS
   const int64_t G = r->scf_opts.grid_chunk > 0 ? r->scf_opts.grid_chunk : 16384;
-  // XC chunk buffers and a V accumulator on each of the 4 concurrent XC
+  // XC chunk buffers and a V accumulator on each of the concurrent XC
   // branches (xc.cu), the grid
-  b += 4 * (6 * nao * G * 8 + 2 * nao * nao * 8) + r->npoint * 4 * 8;
+  b += dfjk::kXcBranches * (6 * nao * G * 8 + 2 * nao * nao * 8) + r->npoint * 4 * 8;
   return b + b / 10 + ((int64_t)256 << 20);
 }
 

@@ -44,7 +44,7 @@ struct XcChunks {
 // chunk's kernels fill only part of the GPU. The accumulators are summed in
 // branch order at the end and the energy partials are per chunk, so the
 // result does not depend on how the branches interleave.
-constexpr int kXcBranches = 4;
+constexpr int kXcBranches = 8;
 
 struct XcBranch {
   DevBuf phi, dphi, X, W;       // [nsig][G] AO values, 3 gradients, Phi P, weighted AO
