@@ -993,6 +993,12 @@ dfjk_status dfjk_destroy(dfjk_ctx* h) {
   cudaSetDevice(h->c.device);
   if (h->c.cublas) cublasDestroy(h->c.cublas);
   if (h->c.cusolver) cusolverDnDestroy(h->c.cusolver);
+  for (int q = 0; q < dfjk::kXcBranches; ++q) {
+    if (h->c.xc_blas[q]) cublasDestroy(h->c.xc_blas[q]);
+    if (h->c.xc_done[q]) cudaEventDestroy(h->c.xc_done[q]);
+    if (h->c.xc_stream[q]) cudaStreamDestroy(h->c.xc_stream[q]);
+  }
+  if (h->c.xc_fork) cudaEventDestroy(h->c.xc_fork);
   const int dev = h->c.device;
   {
     std::lock_guard<std::recursive_mutex> cap(dfjk::capture_mutex());

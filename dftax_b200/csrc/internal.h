@@ -25,11 +25,20 @@ struct PhaseTimer {
 };
 
 
+// The chunks of one XC evaluation run on this many concurrent branches (xc.cu).
+constexpr int kXcBranches = 8;
+
 struct Context {
   int device = 0;
   std::string last_error;
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
+  // streams, join events and cuBLAS handles of the XC branches, made on first
+  // use and kept for the context's life (every SCF of the context reuses them)
+  cudaStream_t xc_stream[kXcBranches] = {};
+  cudaEvent_t xc_done[kXcBranches] = {};
+  cudaEvent_t xc_fork = nullptr;
+  cublasHandle_t xc_blas[kXcBranches] = {};
   DevBuf boys;   // kBoysNgrid x (kBoysNmax+1) doubles
   DevBuf boys_asym;  // 0.5*Gamma(n+1/2), n = 0..kBoysNmax
   // device address of the no-alloc J path's fixed scratch array on this

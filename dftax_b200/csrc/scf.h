@@ -39,20 +39,16 @@ struct XcChunks {
 
 // XC on a point grid (xc.cu)
 // The chunks of one XC evaluation run on kXcBranches concurrent branches
-// (chunk k on branch k % kXcBranches), each with its own buffers, stream and
-// cuBLAS handle (no shared GEMM workspace) and its own V accumulator; one
-// chunk's kernels fill only part of the GPU. The accumulators are summed in
-// branch order at the end and the energy partials are per chunk, so the
-// result does not depend on how the branches interleave.
-constexpr int kXcBranches = 8;
-
+// (chunk k on branch k % kXcBranches), each with its own buffers, and the
+// context's stream and cuBLAS handle of that branch (no shared GEMM
+// workspace), and its own V accumulator; one chunk's kernels fill only part
+// of the GPU. The accumulators are summed in branch order at the end and the
+// energy partials are per chunk, so the result does not depend on how the
+// branches interleave.
 struct XcBranch {
   DevBuf phi, dphi, X, W;       // [nsig][G] AO values, 3 gradients, Phi P, weighted AO
   DevBuf Pc, Vc;                // P on a chunk's AOs, its V block
   DevBuf vr, vg;                // per point: v_rho, v_grad (3)
-  cudaStream_t s = nullptr;
-  cudaEvent_t done = nullptr;
-  cublasHandle_t blas = nullptr;
 };
 
 struct XcWork {
@@ -60,7 +56,6 @@ struct XcWork {
   XcBranch br[kXcBranches];
   DevBuf Vacc;                  // kXcBranches x nao x nao: V accumulated per branch
   DevBuf ered;                  // energy partials per chunk and block
-  cudaEvent_t fork = nullptr;
   // the evaluation's device work as a CUDA graph, captured on the second call
   // with the same arguments and replayed while they stay the same
   cudaGraphExec_t exec = nullptr;
@@ -73,12 +68,6 @@ struct XcWork {
   ~XcWork() {
     if (exec) cudaGraphExecDestroy(exec);
     if (cap) cudaStreamDestroy(cap);
-    for (XcBranch& b : br) {
-      if (b.blas) cublasDestroy(b.blas);
-      if (b.done) cudaEventDestroy(b.done);
-      if (b.s) cudaStreamDestroy(b.s);
-    }
-    if (fork) cudaEventDestroy(fork);
   }
 };
 

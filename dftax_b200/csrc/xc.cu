@@ -571,7 +571,6 @@ void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>&
 static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, const double* w,
                        const double* P, double* Vxc, const XcParams& xp, XcWork& ws,
                        cudaStream_t s) {
-  (void)c;
   const int nao = ov.nao;
   const int64_t nn = (int64_t)nao * nao;
   const XcChunks& ch = ws.ch;
@@ -580,17 +579,19 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
   const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
   const double one = 1.0, zero = 0.0;
   // fork: every branch starts after the caller's prior work on s
-  DFJK_CUDA(cudaEventRecord(ws.fork, s));
-  for (XcBranch& b : ws.br) {
-    DFJK_CUDA(cudaStreamWaitEvent(b.s, ws.fork, 0));
-    DFJK_CUBLAS(cublasSetStream(b.blas, b.s));
+  DFJK_CUDA(cudaEventRecord(c.xc_fork, s));
+  for (int q = 0; q < kXcBranches; ++q) {
+    DFJK_CUDA(cudaStreamWaitEvent(c.xc_stream[q], c.xc_fork, 0));
+    DFJK_CUBLAS(cublasSetStream(c.xc_blas[q], c.xc_stream[q]));
   }
   if (Vxc)
     for (int q = 0; q < kXcBranches; ++q)
-      DFJK_CUDA(cudaMemsetAsync(ws.Vacc.as<double>() + q * nn, 0, nn * sizeof(double), ws.br[q].s));
+      DFJK_CUDA(cudaMemsetAsync(ws.Vacc.as<double>() + q * nn, 0, nn * sizeof(double),
+                                c.xc_stream[q]));
   for (int64_t k = 0; k < nchunk; ++k) {
     XcBranch& b = ws.br[k % kXcBranches];
-    cudaStream_t bs = b.s;
+    cudaStream_t bs = c.xc_stream[k % kXcBranches];
+    cublasHandle_t blas = c.xc_blas[k % kXcBranches];
     double* Vacc = ws.Vacc.as<double>() + (k % kXcBranches) * nn;
     const int64_t g0 = ch.g0[k], ng = ch.ng[k];
     const int nsig = ch.ao_cnt[k], nsh = ch.sh_cnt[k];
@@ -608,7 +609,7 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
         P, nao, map, nsig, b.Pc.as<double>());
     DFJK_LAUNCHED();
     // X (G x nsig, column-major: [k][g]) = Phi Pc
-    DFJK_CUBLAS(cublasDgemm(b.blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nsig, nsig, &one,
+    DFJK_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nsig, nsig, &one,
                             b.phi.as<double>(), (int)G, b.Pc.as<double>(), nsig, &zero,
                             b.X.as<double>(), (int)G));
     rho_kernel<<<(unsigned)((ng + kRhoPts - 1) / kRhoPts), kRhoPts * kRhoLanes, 0, bs>>>(
@@ -625,7 +626,7 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
           G, ng, b.W.as<double>());
       DFJK_LAUNCHED();
       // Vc = Phi^T W, scattered into this branch's V
-      DFJK_CUBLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, nsig, nsig, (int)G, &one,
+      DFJK_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, nsig, nsig, (int)G, &one,
                               b.phi.as<double>(), (int)G, b.W.as<double>(), (int)G, &zero,
                               b.Vc.as<double>(), nsig));
       scatter_v_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, bs>>>(
@@ -634,9 +635,9 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
     }
   }
   // join: s waits for every branch
-  for (XcBranch& b : ws.br) {
-    DFJK_CUDA(cudaEventRecord(b.done, b.s));
-    DFJK_CUDA(cudaStreamWaitEvent(s, b.done, 0));
+  for (int q = 0; q < kXcBranches; ++q) {
+    DFJK_CUDA(cudaEventRecord(c.xc_done[q], c.xc_stream[q]));
+    DFJK_CUDA(cudaStreamWaitEvent(s, c.xc_done[q], 0));
   }
   if (Vxc) {
     symmetrize_sum_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(ws.Vacc.as<double>(),
@@ -664,12 +665,16 @@ double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, co
     b.Vc.ensure(sq);
     b.vr.ensure(G * sizeof(double));
     b.vg.ensure(3 * G * sizeof(double));
-    // streams, events and handles are made here, never during a capture
-    if (!b.s) DFJK_CUDA(cudaStreamCreateWithFlags(&b.s, cudaStreamNonBlocking));
-    if (!b.done) DFJK_CUDA(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
-    if (!b.blas) DFJK_CUBLAS(cublasCreate(&b.blas));
   }
-  if (!ws.fork) DFJK_CUDA(cudaEventCreateWithFlags(&ws.fork, cudaEventDisableTiming));
+  // the context's branch streams, events and handles are made here on first
+  // use, never during a capture
+  Context& cx = const_cast<Context&>(c);
+  for (int q = 0; q < kXcBranches; ++q) {
+    if (!cx.xc_stream[q]) DFJK_CUDA(cudaStreamCreateWithFlags(&cx.xc_stream[q], cudaStreamNonBlocking));
+    if (!cx.xc_done[q]) DFJK_CUDA(cudaEventCreateWithFlags(&cx.xc_done[q], cudaEventDisableTiming));
+    if (!cx.xc_blas[q]) DFJK_CUBLAS(cublasCreate(&cx.xc_blas[q]));
+  }
+  if (!cx.xc_fork) DFJK_CUDA(cudaEventCreateWithFlags(&cx.xc_fork, cudaEventDisableTiming));
   ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
   if (Vxc) ws.Vacc.ensure((size_t)kXcBranches * nao * nao * sizeof(double));
   const void* args[4] = {P, Vxc, pts, w};
