@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=16,
                     help="requests of the seeded Poisson serving stream (0: none)")
     ap.add_argument("--serve-rate", type=float, default=4.0, help="arrivals per second")
+    ap.add_argument("--serve-sweep", default="16",
+                    help="further arrival rates (comma separated) replayed after --serve-rate; "
+                         "empty for none")
     ap.add_argument("--serve-max-water", type=int, default=12,
                     help="largest water cluster of the stream (log-uniform from 3)")
     ap.add_argument("--serve-max-alkane", type=int, default=8,
@@ -474,6 +477,17 @@ def run_ours(args, rank, world, local_rank):
         line["scf"] = scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks)
     if args.serve_requests > 0:
         line["serve"] = serve_measure(args, precs, rank)
+        sweep = []
+        for rate in [float(x) for x in args.serve_sweep.split(",") if x.strip()]:
+            r = serve_measure(args, precs, rank, rate=rate)
+            sweep.append({"rate_per_s": rate,
+                          **{k: r[k] for k in ("value", "p50_latency_s", "p99_latency_s",
+                                               "failed", "max_concurrent")},
+                          "fp64": {k: r["fp64"][k] for k in ("value", "p50_latency_s",
+                                                             "p99_latency_s", "failed")}
+                          if "fp64" in r else None})
+        if sweep:
+            line["serve"]["sweep"] = sweep
     if args.batch > 0:
         line["batch"] = batch_measure(args, precs, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -550,7 +564,7 @@ def _requests(eng, mols, grids, prec, guess=None):
             for (s, x, o, a), g in zip(mols, grids)]
 
 
-def serve_measure(args, precs, rank):
+def serve_measure(args, precs, rank, rate=None):
     """A seeded Poisson stream of SCF requests (water clusters, n log-uniform
     in [3, serve-max-water], and alkanes, n log-uniform in [4, serve-max-alkane],
     half each) through the batch engine: each request is submitted at its
@@ -568,7 +582,8 @@ def serve_measure(args, precs, rank):
     kinds = rng.integers(0, 2, n)
     wn = _loguniform_ints(rng, 3, args.serve_max_water, n)
     an = _loguniform_ints(rng, 4, args.serve_max_alkane, n)
-    gaps = rng.exponential(1.0 / args.serve_rate, n)
+    rate = rate or args.serve_rate
+    gaps = rng.exponential(1.0 / rate, n)
     mols, names = [], []
     for i in range(n):
         name = f"water{wn[i]}" if kinds[i] == 0 else f"alkane{an[i]}"
@@ -610,7 +625,7 @@ def serve_measure(args, precs, rank):
     head = precs[0]
     line = dict(out[head])
     line["precision"] = head
-    line["stream"] = {"requests": n, "rate_per_s": args.serve_rate, "workers": args.workers,
+    line["stream"] = {"requests": n, "rate_per_s": rate, "workers": args.workers,
                       "water_n": [3, args.serve_max_water], "alkane_n": [4, args.serve_max_alkane],
                       "molecules": names, "seed": 50 + rank,
                       "guess": args.guess,
