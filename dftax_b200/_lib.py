@@ -29,7 +29,7 @@ EXPORTS = (
     "dfjk_plan_create", "dfjk_plan_destroy", "dfjk_plan_get_info", "dfjk_build", "dfjk_jk",
     "dfjk_jk_host", "dfjk_energy", "dfjk_eri3c_dense", "dfjk_eri2c_dense", "dfjk_metric_pinv",
     "dfjk_kept_pairs", "dfjk_boys", "dfjk_phase_times", "dfjk_kernel_launches",
-    "dfjk_wait_selftest", "dfjk_energy_grad",
+    "dfjk_wait_selftest", "dfjk_energy_grad", "dfjk_build_batch",
     "dfjk_j_noalloc", "dfjk_trim", "dfjk_plan_long_range", "dfjk_energy_rsh",
     # include/dfscf.h
     "dfscf_default_options", "dfscf_create", "dfscf_destroy", "dfscf_run", "dfscf_get_result",
@@ -143,6 +143,7 @@ def load(path: str | None = None):
         "dfjk_boys": (c_int, [V, V, c_int64, c_int32, V, V]),
         "dfjk_wait_selftest": (c_int, [V, c_int64, V, V]),
         "dfjk_energy_grad": (c_int, [V, V, c_int32, c_double, V, V, V, V]),
+        "dfjk_build_batch": (c_int, [V, c_int32, V]),
         "dfjk_phase_times": (c_int, [V, P(c_double), c_int32]),
         "dfjk_kernel_launches": (c_int64, []),
         "dfjk_j_noalloc": (c_int, [V, V, V, c_int64, V, V]),

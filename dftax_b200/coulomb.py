@@ -202,6 +202,19 @@ class Plan:
         check(self.lib.dfjk_phase_times(self.h, arr, len(_lib.PHASES)), self.ctx.h)
         return dict(zip(_lib.PHASES, list(arr)))
 
+    @staticmethod
+    def build_many(plans, stream=None):
+        """Build several plans of one context together (``dfjk_build_batch``):
+        the 3-center integrals of the small ones share their launches."""
+        plans = list(plans)
+        if not plans:
+            return plans
+        arr = (ctypes.c_void_p * len(plans))(*[p.h.value for p in plans])
+        t = plans[0].torch
+        check(plans[0].lib.dfjk_build_batch(arr, len(plans), _stream_ptr(t, stream)),
+              plans[0].ctx.h)
+        return plans
+
     def build(self, stream=None):
         check(self.lib.dfjk_build(self.h, _stream_ptr(self.torch, stream)), self.ctx.h)
         return self

@@ -771,7 +771,10 @@ int64_t rows_of(const Plan& p, int64_t b, int64_t e) {
   return end_row - p.pair_row0[b];
 }
 
-void build(Plan& p, cudaStream_t s) {
+// Everything a build does before its 3-center rows: the metric factor, the
+// primitive pairs, the workspaces and L's digit planes. Returns the pair
+// chunks of the rows, or no chunks when the plan is streamed (built then).
+static std::vector<std::pair<int64_t, int64_t>> build_begin(Plan& p, cudaStream_t s) {
   p.built = 0;
   // the first build of a plan uses the metric factor computed while the plan
   // was created (same code and inputs); every later build recomputes it
@@ -792,7 +795,6 @@ void build(Plan& p, cudaStream_t s) {
   p.timer.mark(kPhPairs, s);
   launch_pair_setup(p, s);
   p.timer.mark(kPhPairs, s);
-  const bool mixed = p.opts.precision == DFJK_MIXED;
   const int64_t ld = p.naux;
   const int64_t kp = (p.naux + 15) / 16 * 16;
   auto chunks = pair_chunks(p, ld, chunk_budget(p));
@@ -812,25 +814,29 @@ void build(Plan& p, cudaStream_t s) {
     p.ws_bchunk.ensure((size_t)maxrows * p.ldb * sizeof(double));
     ozaki_check(p, s);
     p.built = 1;
-    return;
+    return {};
   }
   p.d_B.ensure((size_t)std::max<int64_t>(p.nrows, 1) * p.ldb * sizeof(double));
-  for (auto& ch : chunks) {
-    const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
-    p.timer.mark(kPhEri3c, s);
-    launch_eri3c_rows(p, ch.first, ch.second, r0, raw.p, ld, false, s);
-    p.timer.mark(kPhEri3c, s);
-    // B[r0:r0+nr, :] = raw (nr x naux) . L (naux x ldb)
-    p.timer.mark(kPhBgemm, s);
-    ozaki_split_raw(p, raw.as<double>(), nr, p.ws_oz_raw.as<int8_t>(), nr * kp,
-                    p.ws_oz_er.as<int>(), s);
-    ozaki_bgemm(p, p.ws_oz_raw.as<int8_t>(), nr * kp, p.ws_oz_er.as<int>(), nr,
-                p.d_B.as<double>() + r0 * p.ldb, s);
-    p.timer.mark(kPhBgemm, s);
-  }
+  return chunks;
+}
+
+// B[r0 : r0 + nr] = raw (nr x naux, in ws_raw) . L on the int8 tensor cores
+static void build_product(Plan& p, int64_t r0, int64_t nr, cudaStream_t s) {
+  const int64_t kp = (p.naux + 15) / 16 * 16;
+  p.timer.mark(kPhBgemm, s);
+  ozaki_split_raw(p, p.ws_raw.as<double>(), nr, p.ws_oz_raw.as<int8_t>(), nr * kp,
+                  p.ws_oz_er.as<int>(), s);
+  ozaki_bgemm(p, p.ws_oz_raw.as<int8_t>(), nr * kp, p.ws_oz_er.as<int>(), nr,
+              p.d_B.as<double>() + r0 * p.ldb, s);
+  p.timer.mark(kPhBgemm, s);
+}
+
+// after the last chunk: the checks and, in mixed precision, the K planes
+static void build_end(Plan& p, cudaStream_t s) {
   // the digit splits flagged any non-finite input (a NaN's digits are
   // finite); float64 plans also scan B for an overflow in the product
   ozaki_check(p, s);
+  const bool mixed = p.opts.precision == DFJK_MIXED;
   if (!mixed) check_finite(p, p.d_B.as<double>(), p.nrows * p.ldb, s, "B");
   if (mixed) {
     p.timer.mark(kPhKplanes, s);
@@ -838,6 +844,38 @@ void build(Plan& p, cudaStream_t s) {
     p.timer.mark(kPhKplanes, s);
   }
   p.built = 1;
+}
+
+void build(Plan& p, cudaStream_t s) {
+  auto chunks = build_begin(p, s);
+  if (p.built) return;   // streamed
+  for (auto& ch : chunks) {
+    const int64_t r0 = p.pair_row0[ch.first], nr = rows_of(p, ch.first, ch.second);
+    p.timer.mark(kPhEri3c, s);
+    launch_eri3c_rows(p, ch.first, ch.second, r0, p.ws_raw.p, p.naux, false, s);
+    p.timer.mark(kPhEri3c, s);
+    build_product(p, r0, nr, s);
+  }
+  build_end(p, s);
+}
+
+void build_batch(const std::vector<Plan*>& ps, cudaStream_t s) {
+  // plans whose rows fit in one chunk share the 3-center launches; the
+  // others (and streamed plans) are built alone
+  std::vector<Plan*> together;
+  for (Plan* p : ps) {
+    if (p->opts.streamed || pair_chunks(*p, p->naux, chunk_budget(*p)).size() > 1) {
+      build(*p, s);
+      continue;
+    }
+    build_begin(*p, s);
+    together.push_back(p);
+  }
+  launch_eri3c_rows_batch(together, s);
+  for (Plan* p : together) {
+    build_product(*p, 0, p->nrows, s);
+    build_end(*p, s);
+  }
 }
 
 void for_each_b_chunk(Plan& p, cudaStream_t s,
@@ -1100,6 +1138,26 @@ dfjk_status dfjk_plan_get_info(const dfjk_plan* pl, dfjk_plan_info* info) {
   info->built = p.built;
   info->precision = p.opts.precision;
   return DFJK_OK;
+}
+
+dfjk_status dfjk_build_batch(dfjk_plan* const* plans, int32_t n, void* stream) {
+  if (!plans || n < 0) return DFJK_ERR_INVALID;
+  if (n == 0) return DFJK_OK;
+  for (int32_t i = 0; i < n; ++i)
+    if (!plans[i]) return DFJK_ERR_INVALID;
+  Context* c = plans[0]->p.ctx;
+  return guard(c, [&] {
+    std::vector<Plan*> ps;
+    for (int32_t i = 0; i < n; ++i) {
+      if (plans[i]->p.ctx != c) fail(DFJK_ERR_INVALID, "plans of one batch need one context");
+      if (plans[i]->p.lr) fail(DFJK_ERR_UNSUPPORTED, "batched builds take no long-range plans");
+      for (int32_t k = 0; k < i; ++k)
+        if (plans[k] == plans[i]) fail(DFJK_ERR_INVALID, "plan %d appears twice", i);
+      ps.push_back(&plans[i]->p);
+    }
+    DFJK_CUDA(cudaSetDevice(c->device));
+    build_batch(ps, st(stream));
+  });
 }
 
 dfjk_status dfjk_build(dfjk_plan* pl, void* stream) {

@@ -20,16 +20,19 @@ namespace dfjk {
 // indices (hermite_r_ct, static_for): their arrays then stay in registers
 constexpr int kStaticM = 6;
 
+// One block of the per-thread kernel: shell pair a.pair_begin + bx, auxiliary
+// slots by * blockDim.x + threadIdx.x (the grid position of a plain launch,
+// or a work-queue entry of a batched one).
 template <int LA, int LB, int LC>
-__global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
+__device__ __forceinline__ void eri3c_block(const Eri3cArgs a, const int64_t bx, const int by) {
   constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, NCC = nc_(LC);
   constexpr int LAB = LA + LB, M = LAB + LC, NH = hcount(LAB), NR = hcount(M), NAB = NA * NB;
   __shared__ double sT[NCC * NC];
   for (int q = threadIdx.x; q < NCC * NC; q += blockDim.x) sT[q] = a.c2s_aux[q];
   __syncthreads();
-  const int slot = blockIdx.y * blockDim.x + threadIdx.x;
+  const int slot = by * blockDim.x + threadIdx.x;
   if (slot >= a.aux_count) return;
-  const int64_t pr = a.pair_begin + blockIdx.x;
+  const int64_t pr = a.pair_begin + bx;
   const int kc = a.aux_sorted[a.aux_begin + slot];
   const double C0 = a.aux.cen[3 * kc], C1 = a.aux.cen[3 * kc + 1], C2 = a.aux.cen[3 * kc + 2];
   const int cp0 = a.aux.prim0[kc], cnp = a.aux.nprim[kc];
@@ -225,8 +228,11 @@ __device__ __forceinline__ double boys_order(int n, double t, const double* __re
   return f;
 }
 
+// One block of the cooperative kernel: shell pair a.pair_begin + bx, its
+// warps taking auxiliary slots by * 4 + warp, then every gy * 4 further.
 template <int LA, int LB, int LC>
-__global__ void __launch_bounds__(128) eri3c_coop_kernel(Eri3cArgs a) {
+__device__ __forceinline__ void eri3c_coop_block(const Eri3cArgs a, const int64_t bx,
+                                                 const int by, const int gy) {
   using S = CoopShape<LA, LB, LC>;
   constexpr int NC = S::NC, NCC = S::NCC, M = S::M, NH = S::NH, NR = S::NR;
   constexpr int NAB = S::NAB, NHP = S::NHP;
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(128) eri3c_coop_kernel(Eri3cArgs a) {
   double* sW = sRb + NR;
   double* sB = sW + NC * NH;
 
-  const int64_t pr = a.pair_begin + blockIdx.x;
+  const int64_t pr = a.pair_begin + bx;
   const int64_t pp0 = a.pair_pp0[pr];
   {
     const double* E = a.esph + (pp0 - a.esph_pp0) * (NAB * NH);
@@ -288,7 +294,7 @@ __global__ void __launch_bounds__(128) eri3c_coop_kernel(Eri3cArgs a) {
   }
   const int i0 = lane, i1 = lane + 32;
 
-  for (int slot = blockIdx.y * 4 + warp; slot < a.aux_count; slot += gridDim.y * 4) {
+  for (int slot = by * 4 + warp; slot < a.aux_count; slot += gy * 4) {
     const int kc = a.aux_sorted[a.aux_begin + slot];
     const int cp0 = a.aux.prim0[kc];
     const double gc = a.aux.pexp[cp0], cc = a.aux.pcoef[cp0];
@@ -402,6 +408,74 @@ __global__ void __launch_bounds__(128) eri3c_coop_kernel(Eri3cArgs a) {
 }
 
 template <int LA, int LB, int LC>
+__global__ void __launch_bounds__(128) eri3c_kernel(Eri3cArgs a) {
+  eri3c_block<LA, LB, LC>(a, blockIdx.x, blockIdx.y);
+}
+
+template <int LA, int LB, int LC>
+__global__ void __launch_bounds__(128) eri3c_coop_kernel(Eri3cArgs a) {
+  eri3c_coop_block<LA, LB, LC>(a, blockIdx.x, blockIdx.y, gridDim.y);
+}
+
+// Several plans' rows of one (LA, LB | LC) class in one launch: a work queue
+// of segments (one plan's run of shell pairs of the class with its
+// arguments), flattened to blocks; block q finds its segment by bisection and
+// computes exactly what the plain launch's block of that segment computes.
+// (A persistent loop over the queue made the compiler's work on these large
+// bodies grow sevenfold, so each queue entry is a block.)
+struct Eri3cBatch {
+  const Eri3cArgs* seg;      // per segment (device)
+  const int64_t* blk0;       // first queue entry of each segment, [nseg + 1]
+  const int* ydim;           // y extent of each segment's plain grid
+  int nseg;
+  int64_t total;             // queue entries = blocks of the launch
+};
+
+__device__ __forceinline__ int batch_segment(const Eri3cBatch& b, int64_t q) {
+  int lo = 0, hi = b.nseg;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (b.blk0[mid] <= q) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <int LA, int LB, int LC>
+__global__ void __launch_bounds__(128) eri3c_batch_kernel(Eri3cBatch b) {
+  const int64_t q = blockIdx.x;
+  const int sg = batch_segment(b, q);
+  const int64_t local = q - b.blk0[sg];
+  const int y = b.ydim[sg];
+  eri3c_block<LA, LB, LC>(b.seg[sg], local / y, (int)(local % y));
+}
+
+// the classes whose rows are batched: those below the cooperative kernel's
+// size (heavier classes keep one launch per plan; duplicating their large
+// bodies would double the library's build time)
+template <int LA, int LB, int LC>
+inline bool launch_one_batch(unsigned blocks, cudaStream_t s, const Eri3cBatch& b) {
+  if constexpr (LA + LB + LC < kCoopM) {
+    eri3c_batch_kernel<LA, LB, LC><<<blocks, 128, 0, s>>>(b);
+    return true;
+  } else {
+    return false;
+  }
+}
+
+template <int LA, int LB>
+inline bool launch_lc_batch(int lc, unsigned blocks, cudaStream_t s, const Eri3cBatch& b) {
+  switch (lc) {
+    case 0: return launch_one_batch<LA, LB, 0>(blocks, s, b);
+    case 1: return launch_one_batch<LA, LB, 1>(blocks, s, b);
+    case 2: return launch_one_batch<LA, LB, 2>(blocks, s, b);
+    case 3: return launch_one_batch<LA, LB, 3>(blocks, s, b);
+    case 4: return launch_one_batch<LA, LB, 4>(blocks, s, b);
+    default: return false;
+  }
+}
+
+template <int LA, int LB, int LC>
 inline void launch_one(dim3 grid, cudaStream_t s, const Eri3cArgs& a) {
   if constexpr (LA + LB + LC >= kCoopM) {
     if (a.uncontracted) {
@@ -438,6 +512,37 @@ bool launch_eri3c_30(int lc, dim3 grid, cudaStream_t s, const Eri3cArgs& a);
 bool launch_eri3c_31(int lc, dim3 grid, cudaStream_t s, const Eri3cArgs& a);
 bool launch_eri3c_32(int lc, dim3 grid, cudaStream_t s, const Eri3cArgs& a);
 bool launch_eri3c_33(int lc, dim3 grid, cudaStream_t s, const Eri3cArgs& a);
+
+#define DFJK_ERI3C_BATCH_DECL(A, B) \
+  bool launch_eri3c_batch_##A##B(int lc, unsigned blocks, cudaStream_t s, const Eri3cBatch& b);
+DFJK_ERI3C_BATCH_DECL(0, 0)
+DFJK_ERI3C_BATCH_DECL(1, 0)
+DFJK_ERI3C_BATCH_DECL(1, 1)
+DFJK_ERI3C_BATCH_DECL(2, 0)
+DFJK_ERI3C_BATCH_DECL(2, 1)
+DFJK_ERI3C_BATCH_DECL(2, 2)
+DFJK_ERI3C_BATCH_DECL(3, 0)
+DFJK_ERI3C_BATCH_DECL(3, 1)
+DFJK_ERI3C_BATCH_DECL(3, 2)
+DFJK_ERI3C_BATCH_DECL(3, 3)
+#undef DFJK_ERI3C_BATCH_DECL
+
+inline bool launch_eri3c_batch(int l1, int l2, int lc, unsigned blocks, cudaStream_t s,
+                               const Eri3cBatch& b) {
+  switch (l1 * 4 + l2) {
+    case 0: return launch_eri3c_batch_00(lc, blocks, s, b);
+    case 4: return launch_eri3c_batch_10(lc, blocks, s, b);
+    case 5: return launch_eri3c_batch_11(lc, blocks, s, b);
+    case 8: return launch_eri3c_batch_20(lc, blocks, s, b);
+    case 9: return launch_eri3c_batch_21(lc, blocks, s, b);
+    case 10: return launch_eri3c_batch_22(lc, blocks, s, b);
+    case 12: return launch_eri3c_batch_30(lc, blocks, s, b);
+    case 13: return launch_eri3c_batch_31(lc, blocks, s, b);
+    case 14: return launch_eri3c_batch_32(lc, blocks, s, b);
+    case 15: return launch_eri3c_batch_33(lc, blocks, s, b);
+    default: return false;
+  }
+}
 
 inline bool launch_eri3c(int l1, int l2, int lc, dim3 grid, cudaStream_t s, const Eri3cArgs& a) {
   switch (l1 * 4 + l2) {

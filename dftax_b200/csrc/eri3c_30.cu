@@ -7,4 +7,8 @@ bool launch_eri3c_30(int lc, dim3 grid, cudaStream_t s, const Eri3cArgs& a) {
   return launch_lc<3, 0>(lc, grid, s, a);
 }
 
+bool launch_eri3c_batch_30(int lc, unsigned blocks, cudaStream_t s, const Eri3cBatch& b) {
+  return launch_lc_batch<3, 0>(lc, blocks, s, b);
+}
+
 }  // namespace dfjk

@@ -146,6 +146,14 @@ void for_each_b_chunk(Plan& p, cudaStream_t s,
 void boys_table_host(std::vector<double>& tbl, std::vector<double>& asym);
 void launch_boys(const Context& c, const double* t, int64_t n, int nmax, double* out, cudaStream_t s);
 void launch_pair_setup(Plan& p, cudaStream_t s);
+// Every row of several plans (each into its ws_raw, ld = naux) with one
+// persistent launch per (l1, l2 | lc) class over a work queue spanning the
+// plans.
+void launch_eri3c_rows_batch(const std::vector<Plan*>& ps, cudaStream_t s);
+// Builds several plans of one context: the 3-center rows of the plans whose
+// rows fit in one chunk share their launches (launch_eri3c_rows_batch); the
+// others are built one by one.
+void build_batch(const std::vector<Plan*>& ps, cudaStream_t s);
 void launch_eri3c_rows(Plan& p, int64_t pair_begin, int64_t pair_end, int64_t row_base,
                        void* out, int64_t ld, bool f32, cudaStream_t s);
 void launch_eri2c(Plan& p, double* out, int64_t ld, cudaStream_t s);

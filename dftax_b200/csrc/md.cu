@@ -17,6 +17,8 @@
 #include "internal.h"
 
 #include <cmath>
+#include <map>
+#include <tuple>
 
 namespace dfjk {
 
@@ -454,6 +456,102 @@ void launch_eri3c_rows(Plan& p, int64_t pair_begin, int64_t pair_end, int64_t ro
         DFJK_LAUNCHED();
       }
     }
+  }
+}
+
+void launch_eri3c_rows_batch(const std::vector<Plan*>& ps, cudaStream_t s) {
+  if (ps.empty()) return;
+  const Context& c = *ps[0]->ctx;
+  auto single = [](const std::vector<int>& np) {
+    for (int n : np)
+      if (n != 1) return false;
+    return true;
+  };
+  // segments per light (l1, l2 | lc) class, in plan order
+  struct Group {
+    std::vector<Eri3cArgs> seg;
+    std::vector<int64_t> blk0{0};
+    std::vector<int> ydim;
+  };
+  std::map<std::tuple<int, int, int>, Group> groups;
+  for (Plan* pp : ps) {
+    Plan& p = *pp;
+    const int uncontracted = single(p.orb.nprim) && single(p.aux.nprim) ? 1 : 0;
+    for (const ClassRange& cr : p.classes) {
+      if (cr.count == 0) continue;
+      for (int lc = 0; lc <= p.aux.lmax; ++lc) {
+        if (p.aux_lcount[lc] == 0) continue;
+        Eri3cArgs a;
+        a.pair_row0 = p.d_pair_row0.as<int64_t>();
+        a.pair_pp0 = p.d_pair_pp0.as<int64_t>();
+        a.pair_npp = p.d_pair_npp.as<int>();
+        a.pp_P = p.d_pp_P.as<double>();
+        a.pp_g = p.d_pp_g.as<double>();
+        a.pp_pref = p.d_pp_pref.as<double>();
+        a.esph = p.d_esph.as<double>() + cr.esph_off;
+        a.esph_pp0 = cr.pp_begin;
+        a.aux_sorted = p.d_aux_sorted.as<int>();
+        a.aux = view(p.aux);
+        a.c2s_aux = p.c2s_aux.dev.as<double>() + p.c2s_aux.off[lc];
+        a.boys = c.boys.as<double>();
+        a.boys_asym = c.boys_asym.as<double>();
+        a.aux_begin = p.aux_lbegin[lc];
+        a.aux_count = p.aux_lcount[lc];
+        a.col_base = p.aux_col0[p.aux_order[p.aux_lbegin[lc]]];
+        a.row_base = 0;
+        a.ld = p.naux;
+        a.out = p.ws_raw.p;
+        a.out_f32 = 0;
+        a.omega = p.atten;
+        a.uncontracted = uncontracted;
+        a.pair_begin = cr.begin;
+        const int y = (a.aux_count + 127) / 128;
+        if (cr.l1 + cr.l2 + lc >= kCoopM) {
+          // heavy classes keep the plain launch of this plan (launch_one picks
+          // the cooperative kernel for uncontracted shells)
+          if (!launch_eri3c(cr.l1, cr.l2, lc, dim3((unsigned)cr.count, (unsigned)y), s, a))
+            fail(DFJK_ERR_UNSUPPORTED, "3-center class (%d,%d|%d) not compiled", cr.l1, cr.l2, lc);
+          DFJK_LAUNCHED();
+          continue;
+        }
+        Group& g = groups[{cr.l1, cr.l2, lc}];
+        g.seg.push_back(a);
+        g.ydim.push_back(y);
+        g.blk0.push_back(g.blk0.back() + cr.count * (int64_t)y);
+      }
+    }
+  }
+  // the queue tables: one set of buffers per group, freed into the device
+  // cache (whose reuse waits for the device) when this function returns; the
+  // pageable host tables are staged by the time each copy returns
+  std::vector<DevBuf> keep(groups.size() * 3);
+  size_t k = 0;
+  for (auto& kv : groups) {
+    const int l1 = std::get<0>(kv.first), l2 = std::get<1>(kv.first), lc = std::get<2>(kv.first);
+    Group& g = kv.second;
+    DevBuf& dseg = keep[k++];
+    DevBuf& dblk = keep[k++];
+    DevBuf& dy = keep[k++];
+    dseg.alloc(g.seg.size() * sizeof(Eri3cArgs));
+    DFJK_CUDA(cudaMemcpyAsync(dseg.p, g.seg.data(), g.seg.size() * sizeof(Eri3cArgs),
+                              cudaMemcpyHostToDevice, s));
+    dblk.alloc(g.blk0.size() * sizeof(int64_t));
+    DFJK_CUDA(cudaMemcpyAsync(dblk.p, g.blk0.data(), g.blk0.size() * sizeof(int64_t),
+                              cudaMemcpyHostToDevice, s));
+    dy.alloc(g.ydim.size() * sizeof(int));
+    DFJK_CUDA(cudaMemcpyAsync(dy.p, g.ydim.data(), g.ydim.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+    Eri3cBatch b;
+    b.seg = dseg.as<Eri3cArgs>();
+    b.blk0 = dblk.as<int64_t>();
+    b.ydim = dy.as<int>();
+    b.nseg = (int)g.seg.size();
+    b.total = g.blk0.back();
+    const unsigned blocks = (unsigned)b.total;   // one block per queue entry
+    if (blocks == 0) continue;
+    if (!launch_eri3c_batch(l1, l2, lc, blocks, s, b))
+      fail(DFJK_ERR_UNSUPPORTED, "3-center class (%d,%d|%d) not compiled", l1, l2, lc);
+    DFJK_LAUNCHED();
   }
 }
 

@@ -123,6 +123,17 @@ dfjk_status dfjk_plan_get_info(const dfjk_plan* plan, dfjk_plan_info* info);
  * Host-synchronizing (the kept-direction count sizes B). */
 dfjk_status dfjk_build(dfjk_plan* plan, void* stream);
 
+/* dfjk_build of n plans of one context (molecules of any sizes): the 3-center
+ * integrals of every plan whose rows fit in one staging chunk are computed
+ * in shared launches, one persistent launch per (l1, l2 | lc) integral class
+ * whose blocks walk a work queue of (plan, run of shell pairs) segments, so
+ * small molecules do not each pay a launch per class; then each plan's
+ * B = (ij|P) L. Larger and streamed plans are built as dfjk_build builds
+ * them. Every plan ends exactly as its own dfjk_build leaves it (the same
+ * blocks compute the same rows). No counterpart in dftax, whose batched
+ * solver (dftax/ks/batched.py:82-304) vmaps one molecule's conformers. */
+dfjk_status dfjk_build_batch(dfjk_plan* const* plans, int32_t n, void* stream);
+
 /* J and K of the density D = C diag(w) C^T (w == NULL: all ones), with
  * C [nao][ncol] row-major on the device. J, K: [nao][nao] device outputs.
  * J = sum_PQ (mn|P) V+_PQ (P|D), K = sum_PQ (ml|P) V+_PQ (ns|Q) D_ls
