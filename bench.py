@@ -70,6 +70,8 @@ def parse():
                     help="also solve a batch of this many water clusters (64: the 64-cluster "
                          "batch, n log-uniform in [3, 40])")
     ap.add_argument("--workers", type=int, default=4, help="concurrent solves of the engine")
+    ap.add_argument("--build-batch", type=int, default=64,
+                    help="water clusters of the batched-build measurement (0: off)")
     ap.add_argument("--guess", default="sad", choices=["sad", "core"],
                     help="SCF starting density of the SCF, serving and batch measurements")
     ap.add_argument("--screen", type=float, default=0.0,
@@ -490,6 +492,8 @@ def run_ours(args, rank, world, local_rank):
             line["serve"]["sweep"] = sweep
     if args.batch > 0:
         line["batch"] = batch_measure(args, precs, rank)
+    if args.build_batch > 0:
+        line["build_batch"] = build_batch_measure(args, precs, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         secs, parts, n = cpu_full_builds(args.workload, 1)
         line["cpu_baseline"] = {"value": round(1.0 / secs[0], 6), "unit": UNIT, "cores": n,
@@ -635,6 +639,60 @@ def serve_measure(args, precs, rank, rate=None):
         both = [i for i in range(n) if ok_mask[head][i] and ok_mask["fp64"][i]]
         line["max_abs_dE_vs_fp64_Ha"] = (float(np.max(np.abs(
             np.array(energies[head])[both] - np.array(energies["fp64"])[both]))) if both else None)
+    return line
+
+
+def build_batch_measure(args, precs, rank):
+    """DF builds of many small molecules: water clusters, n log-uniform in
+    [3, 12] (seeded), plans made up front (untimed); the same builds timed one
+    plan after another (dfjk_build each) and all together (dfjk_build_batch:
+    one launch per light integral class for every molecule). CUDA events on
+    the stream around each way, after one untimed round."""
+    import torch
+
+    from dftax_b200 import Plan, systems
+    from dftax_b200._lib import load
+
+    lib = load()
+    rng = np.random.default_rng(12 + rank)
+    ns = _loguniform_ints(rng, 3, 12, args.build_batch)
+    out = {}
+    for prec in precs:
+        plans = []
+        for i, n in enumerate(ns):
+            _, _, orb, aux, _ = systems.workload(f"water{n}", seed=3000 + i)
+            plans.append(Plan(orb, aux, precision=prec))
+        res = {}
+        for way in ("single", "batched"):
+            def run():
+                if way == "single":
+                    for p in plans:
+                        p.build()
+                else:
+                    Plan.build_many(plans)
+            run()
+            torch.cuda.synchronize()
+            k0 = lib.dfjk_kernel_launches()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            res[way] = {"value": round(len(plans) / (ms / 1e3), 3), "unit": "builds/s",
+                        "ms": round(ms, 2),
+                        "kernel_launches": int(lib.dfjk_kernel_launches() - k0)}
+        res["speedup"] = round(res["single"]["ms"] / res["batched"]["ms"], 3)
+        for p in plans:
+            p.close()
+        out[prec] = res
+    head = precs[0]
+    line = dict(out[head])
+    line["precision"] = head
+    line["molecules"] = {"count": int(args.build_batch), "n": ns.tolist(), "seed": 12 + rank,
+                         "what": "one DF build (metric, 3-center rows, B) per water cluster"}
+    if "fp64" in out and head != "fp64":
+        line["fp64"] = out["fp64"]
     return line
 
 

@@ -78,7 +78,8 @@ class ScfOptions(ctypes.Structure):
                 ("e_tol", c_double), ("d_tol", c_double), ("lindep", c_double),
                 ("level_shift", c_double), ("rho_thresh", c_double), ("ao_thresh", c_double),
                 ("max_iter", c_int32),
-                ("diis_space", c_int32), ("grid_chunk", c_int64)]
+                ("diis_space", c_int32), ("grid_chunk", c_int64), ("xc_streams", c_int32),
+                ("reserved", c_int32)]
 
 
 class ScfResult(ctypes.Structure):

@@ -113,9 +113,10 @@ int64_t estimate(const dfbatch_request* r) {
   const int64_t diis = r->scf_opts.diis_space > 0 ? r->scf_opts.diis_space : 8;
   b += (14 + 2 * diis) * nao * nao * 8;                          // SCF matrices, DIIS
   const int64_t G = r->scf_opts.grid_chunk > 0 ? r->scf_opts.grid_chunk : 16384;
-  // XC chunk buffers and a V accumulator on each of the concurrent XC
-  // branches (xc.cu), the grid
-  b += dfjk::kXcBranches * (6 * nao * G * 8 + 2 * nao * nao * 8) + r->npoint * 4 * 8;
+  // XC chunk buffers and a V accumulator on each of the solve's XC streams
+  // (one unless the request asks for more: xc.cu), the grid
+  const int64_t nbr = r->scf_opts.xc_streams > 0 ? r->scf_opts.xc_streams : 1;
+  b += nbr * (6 * nao * G * 8 + 2 * nao * nao * 8) + r->npoint * 4 * 8;
   return b + b / 10 + ((int64_t)256 << 20);
 }
 
@@ -146,6 +147,9 @@ void run_job(dfjk_ctx* ctx, cudaStream_t s, Job& j) {
   dfjk_status st = DFJK_OK;
   std::string msg;
   try {
+    // the engine's solves overlap one another: each runs its XC chunks on one
+    // stream unless the request asks otherwise
+    if (j.sopts.xc_streams == 0) j.sopts.xc_streams = 1;
     check(dfjk_plan_create(ctx, &j.orb.b, &j.aux.b, &j.popts, &plan));
     check(dfjk_build(plan, s));
     check(dfscf_create(plan, j.natom, j.xyz.data(), j.charge.data(), j.npoint,

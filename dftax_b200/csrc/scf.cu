@@ -437,6 +437,7 @@ void dfscf_default_options(dfscf_options* o) {
   o->max_iter = 128;
   o->diis_space = 8;
   o->grid_chunk = 0;
+  o->xc_streams = 0;
 }
 
 dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
@@ -461,6 +462,9 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     if (opts) f->o = *opts;
     else dfscf_default_options(&f->o);
     if (f->o.diis_space < 1 || f->o.max_iter < 0) fail(DFJK_ERR_INVALID, "invalid SCF options");
+    if (f->o.xc_streams < 0 || f->o.xc_streams > kXcBranches)
+      fail(DFJK_ERR_INVALID, "xc_streams must be 0..%d", kXcBranches);
+    f->xcw.nbr = f->o.xc_streams > 0 ? f->o.xc_streams : kXcBranches;
     for (int64_t i = 0; i < 3 * (int64_t)natom; ++i)
       if (!std::isfinite(atom_xyz[i])) fail(DFJK_ERR_NUMERIC, "non-finite atom coordinate");
     for (int64_t i = 0; i < 3 * npoint; ++i)

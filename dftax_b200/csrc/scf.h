@@ -53,6 +53,7 @@ struct XcBranch {
 
 struct XcWork {
   XcChunks ch;
+  int nbr = kXcBranches;        // branches in use, 1..kXcBranches
   XcBranch br[kXcBranches];
   DevBuf Vacc;                  // kXcBranches x nao x nao: V accumulated per branch
   DevBuf ered;                  // energy partials per chunk and block

@@ -578,21 +578,22 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
   const int64_t nchunk = (int64_t)ch.g0.size();
   const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
   const double one = 1.0, zero = 0.0;
+  const int nb = std::min(std::max(ws.nbr, 1), kXcBranches);
   // fork: every branch starts after the caller's prior work on s
   DFJK_CUDA(cudaEventRecord(c.xc_fork, s));
-  for (int q = 0; q < kXcBranches; ++q) {
+  for (int q = 0; q < nb; ++q) {
     DFJK_CUDA(cudaStreamWaitEvent(c.xc_stream[q], c.xc_fork, 0));
     DFJK_CUBLAS(cublasSetStream(c.xc_blas[q], c.xc_stream[q]));
   }
   if (Vxc)
-    for (int q = 0; q < kXcBranches; ++q)
+    for (int q = 0; q < nb; ++q)
       DFJK_CUDA(cudaMemsetAsync(ws.Vacc.as<double>() + q * nn, 0, nn * sizeof(double),
                                 c.xc_stream[q]));
   for (int64_t k = 0; k < nchunk; ++k) {
-    XcBranch& b = ws.br[k % kXcBranches];
-    cudaStream_t bs = c.xc_stream[k % kXcBranches];
-    cublasHandle_t blas = c.xc_blas[k % kXcBranches];
-    double* Vacc = ws.Vacc.as<double>() + (k % kXcBranches) * nn;
+    XcBranch& b = ws.br[k % nb];
+    cudaStream_t bs = c.xc_stream[k % nb];
+    cublasHandle_t blas = c.xc_blas[k % nb];
+    double* Vacc = ws.Vacc.as<double>() + (k % nb) * nn;
     const int64_t g0 = ch.g0[k], ng = ch.ng[k];
     const int nsig = ch.ao_cnt[k], nsh = ch.sh_cnt[k];
     const int* map = ch.d_ao_map.as<int>() + ch.ao_off[k];
@@ -635,13 +636,13 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
     }
   }
   // join: s waits for every branch
-  for (int q = 0; q < kXcBranches; ++q) {
+  for (int q = 0; q < nb; ++q) {
     DFJK_CUDA(cudaEventRecord(c.xc_done[q], c.xc_stream[q]));
     DFJK_CUDA(cudaStreamWaitEvent(s, c.xc_done[q], 0));
   }
   if (Vxc) {
     symmetrize_sum_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(ws.Vacc.as<double>(),
-                                                                        kXcBranches, nao, Vxc);
+                                                                        nb, nao, Vxc);
     DFJK_LAUNCHED();
   }
 }
@@ -656,7 +657,8 @@ double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, co
   const int64_t nblk = (G + kPtThreads - 1) / kPtThreads;
   const int64_t plane_max = (int64_t)std::max(ch.max_ao, 1) * G;
   const size_t sq = (size_t)std::max(ch.max_ao, 1) * std::max(ch.max_ao, 1) * sizeof(double);
-  for (XcBranch& b : ws.br) {
+  for (int q = 0; q < std::min(std::max(ws.nbr, 1), kXcBranches); ++q) {
+    XcBranch& b = ws.br[q];
     b.phi.ensure(plane_max * sizeof(double));
     b.dphi.ensure(3 * plane_max * sizeof(double));
     b.X.ensure(plane_max * sizeof(double));
@@ -676,7 +678,7 @@ double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, co
   }
   if (!cx.xc_fork) DFJK_CUDA(cudaEventCreateWithFlags(&cx.xc_fork, cudaEventDisableTiming));
   ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
-  if (Vxc) ws.Vacc.ensure((size_t)kXcBranches * nao * nao * sizeof(double));
+  if (Vxc) ws.Vacc.ensure((size_t)std::max(ws.nbr, 1) * nao * nao * sizeof(double));
   const void* args[4] = {P, Vxc, pts, w};
   const bool same = std::equal(args, args + 4, ws.g_args);
   if (ws.exec && same) {

@@ -61,7 +61,7 @@ class KS:
     def __init__(self, symbols, coords_bohr, basis: BasisData, *, coulomb: DFSpec, xc="PBE0",
                  grid=None, charges=None, device: int = 0, diis_space: int = 8,
                  lindep_thresh: float = 1e-7, plan: Plan | None = None,
-                 ao_thresh: float = 1e-14, grid_chunk: int = 0):
+                 ao_thresh: float = 1e-14, grid_chunk: int = 0, xc_streams: int = 0):
         if xc not in XC_FUNCTIONALS:
             raise ValueError(f"xc must be one of {sorted(XC_FUNCTIONALS)}")
         if not isinstance(coulomb, DFSpec) or not isinstance(coulomb.auxbasis, BasisData):
@@ -97,6 +97,7 @@ class KS:
                                                              device=self.ctx.device)
         self._diis, self._lindep = diis_space, lindep_thresh
         self._ao_thresh, self._grid_chunk = float(ao_thresh), int(grid_chunk)
+        self._xc_streams = int(xc_streams)   # 0: 8 concurrent XC streams; the batch engine uses 1
         self.h = ctypes.c_void_p()
         self._create()
 
@@ -111,6 +112,7 @@ class KS:
         o.lindep = float(self._lindep)
         o.ao_thresh = self._ao_thresh
         o.grid_chunk = self._grid_chunk
+        o.xc_streams = self._xc_streams
         self._opts = o
         _lib.check(self.lib.dfscf_create(self.plan.h, len(self.charges), self.coords.ctypes.data,
                                          self.charges.ctypes.data, len(self.grid_weights),

@@ -44,6 +44,10 @@ typedef struct {
   int64_t grid_chunk;   /* grid points per XC chunk, spatially sorted (0: chosen by
                            timing 4096, 8192 and 16384 on the first molecule of each
                            size; the choice is kept for the process)                   */
+  int32_t xc_streams;   /* concurrent streams the XC chunks run on, 1..8 (0: 8); the
+                           batch engine runs its solves, which already overlap one
+                           another, with 1                                             */
+  int32_t reserved;
 } dfscf_options;
 
 typedef struct {

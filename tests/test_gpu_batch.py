@@ -3,7 +3,8 @@
   * every result of a batch of molecules of uneven size (monomer to (H2O)_5,
     ethane) equals the same molecule solved alone: |dE| <= 1e-10 Ha and the
     density to 1e-8 (the same kernels with fixed-order reductions run either
-    way);
+    way; the engine runs each solve's XC on one stream, so the solo solves
+    here do too);
   * with room for several, solves overlap in time, and the estimated bytes of
     the solves running at once never exceed the budget;
   * with room for one, they run one after another;
@@ -47,7 +48,7 @@ def solo(grid):
 
     res = []
     for sym, xyz, orb, aux in molecules():
-        ks = KS(sym, xyz, orb, coulomb=df(aux), grid=grid)
+        ks = KS(sym, xyz, orb, coulomb=df(aux), grid=grid, xc_streams=1)
         r = scf(ks)
         res.append((r.e_tot, r.P[0]))
         ks.close()
@@ -159,7 +160,7 @@ def test_stream_with_buffer_reuse_across_workers(grid):
     mols = [systems.workload(nm, seed=7)[:4] for nm in names]
     solo = []
     for sym, xyz, orb, aux in mols:
-        ks = KS(sym, xyz, orb, coulomb=df(aux, precision="mixed"), grid=grid)
+        ks = KS(sym, xyz, orb, coulomb=df(aux, precision="mixed"), grid=grid, xc_streams=1)
         solo.append(scf(ks).e_tot)
         ks.close()
         ks.plan.close()

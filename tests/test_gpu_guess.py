@@ -62,7 +62,7 @@ def test_batch_with_sad_equals_solo():
     mols = [systems.workload(nm, seed=4)[:4] for nm in ("water3", "alkane3", "water2")]
     solo = []
     for sym, xyz, orb, aux in mols:
-        ks = KS(sym, xyz, orb, coulomb=df(aux), grid=g)
+        ks = KS(sym, xyz, orb, coulomb=df(aux), grid=g, xc_streams=1)   # as the engine runs it
         solo.append(scf(ks, guess="sad").e_tot)
         ks.close()
     res = scf_batch(mols, grid=g, workers=3, guess="sad")
