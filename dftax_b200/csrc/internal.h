@@ -39,6 +39,9 @@ struct Context {
   cudaEvent_t xc_done[kXcBranches] = {};
   cudaEvent_t xc_fork = nullptr;
   cublasHandle_t xc_blas[kXcBranches] = {};
+  // each branch handle's GEMM workspace, set explicitly (cublasSetWorkspace)
+  // so cuBLAS never allocates one itself around a graph capture
+  DevBuf xc_ws[kXcBranches];
   DevBuf boys;   // kBoysNgrid x (kBoysNmax+1) doubles
   DevBuf boys_asym;  // 0.5*Gamma(n+1/2), n = 0..kBoysNmax
   // device address of the no-alloc J path's fixed scratch array on this

@@ -32,6 +32,7 @@ namespace dfjk {
 namespace {
 
 constexpr int kAoThreads = 128;
+constexpr size_t kXcBlasWorkspace = (size_t)8 << 20;   // per XC branch cuBLAS handle
 constexpr int kPtThreads = 256;
 
 // ---------------------------------------------------------------------------
@@ -584,6 +585,8 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
   for (int q = 0; q < nb; ++q) {
     DFJK_CUDA(cudaStreamWaitEvent(c.xc_stream[q], c.xc_fork, 0));
     DFJK_CUBLAS(cublasSetStream(c.xc_blas[q], c.xc_stream[q]));
+    // (setting the stream resets the workspace: give it back each time)
+    DFJK_CUBLAS(cublasSetWorkspace(c.xc_blas[q], c.xc_ws[q].p, kXcBlasWorkspace));
   }
   if (Vxc)
     for (int q = 0; q < nb; ++q)
@@ -675,6 +678,7 @@ double xc_energy_fock(const Context& c, const OrbView& ov, const double* pts, co
     if (!cx.xc_stream[q]) DFJK_CUDA(cudaStreamCreateWithFlags(&cx.xc_stream[q], cudaStreamNonBlocking));
     if (!cx.xc_done[q]) DFJK_CUDA(cudaEventCreateWithFlags(&cx.xc_done[q], cudaEventDisableTiming));
     if (!cx.xc_blas[q]) DFJK_CUBLAS(cublasCreate(&cx.xc_blas[q]));
+    cx.xc_ws[q].ensure(kXcBlasWorkspace);
   }
   if (!cx.xc_fork) DFJK_CUDA(cudaEventCreateWithFlags(&cx.xc_fork, cudaEventDisableTiming));
   ws.ered.ensure((size_t)std::max<int64_t>(nchunk, 1) * nblk * sizeof(double));
