@@ -469,9 +469,17 @@ static void syrk_fp64(Plan& p, const double* X, int64_t kt, double sign, bool be
 }
 
 // K (+)= sign * X X^T for the selected columns of C (scaled by sqrt|w|)
+// fuse (streamed plans only, may be null): gamma = B^T dvec is also summed
+// in the first pass over B's chunks (one rebuild of B fewer per J/K call);
+// its dvec is cleared once gamma is done.
+struct GammaFuse {
+  const double* dvec = nullptr;
+  double* gamma = nullptr;
+};
+
 static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol,
                          const std::vector<int>& sel, double sign, bool first, double* K,
-                         cudaStream_t s) {
+                         cudaStream_t s, GammaFuse* fuse = nullptr) {
   Context& c = *p.ctx;
   const int64_t nao = p.nao, nsel = (int64_t)sel.size();
   if (nsel == 0) return;
@@ -510,7 +518,10 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
       DFJK_CUDA(cudaMemsetAsync(X.p, 0, (size_t)nao * n * nsel * sizeof(double), s));
       p.ws_kb.ensure(nao * sizeof(int));
       p.ws_ke.ensure(nao * sizeof(int));
+      const bool with_gamma = fuse && fuse->dvec;
+      if (with_gamma) DFJK_CUDA(cudaMemsetAsync(fuse->gamma, 0, p.ldb * sizeof(double), s));
       for_each_b_chunk(p, s, [&](int64_t r0, int64_t nr, const double* Bc) {
+        if (with_gamma && nr > 0) gamma_rows(p, Bc, nr, fuse->dvec + r0, fuse->gamma, true, s);
         list_bounds_kernel<<<(unsigned)((nao + 255) / 256), 256, 0, s>>>(
             p.d_kptr.as<int>(), p.d_krow.as<int>(), nao, r0, r0 + nr, p.ws_kb.as<int>(),
             p.ws_ke.as<int>());
@@ -521,6 +532,7 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
                                                    X.as<double>());
         DFJK_LAUNCHED();
       });
+      if (with_gamma) fuse->dvec = nullptr;   // gamma is complete
     } else if (oz) {
       if (x0 == 0) ozaki_prepare_c(p, Cp.as<double>(), nsel, s);
       ozaki_k1(p, nsel, x0, n, X.as<double>(), s);   // int8 tensor cores, exact accumulation
@@ -544,7 +556,7 @@ static void k_accumulate(Plan& p, const double* C, const double* w, int64_t ncol
 }
 
 static void k_compute(Plan& p, const double* C, const double* w, int64_t ncol, double* K,
-                      cudaStream_t s) {
+                      cudaStream_t s, GammaFuse* fuse = nullptr) {
   std::vector<int> pos, neg;
   if (w) {
     std::vector<double> hw(ncol);
@@ -562,8 +574,8 @@ static void k_compute(Plan& p, const double* C, const double* w, int64_t ncol, d
     DFJK_CUDA(cudaMemsetAsync(K, 0, (size_t)p.nao * p.nao * sizeof(double), s));
     return;
   }
-  k_accumulate(p, C, w, ncol, pos, 1.0, true, K, s);
-  k_accumulate(p, C, w, ncol, neg, -1.0, pos.empty(), K, s);
+  k_accumulate(p, C, w, ncol, pos, 1.0, true, K, s, fuse);
+  k_accumulate(p, C, w, ncol, neg, -1.0, pos.empty(), K, s, fuse);
   const int64_t n = p.nao;
   symmetrize_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(K, n);
   DFJK_LAUNCHED();
@@ -583,6 +595,16 @@ void jk_compute(Plan& p, const double* C, const double* w, int64_t ncol, double*
           C, w, ncol, p.d_row_m.as<int>(), p.d_row_n.as<int>(), p.d_row_w.as<int8_t>(), p.nrows,
           dvec.as<double>());
       DFJK_LAUNCHED();
+    }
+    if (p.opts.streamed && K) {
+      // one pass over B's chunks gives gamma and the K half transform; J
+      // takes a second
+      GammaFuse fuse{dvec.as<double>(), gamma.as<double>()};
+      k_compute(p, C, w, ncol, K, s, &fuse);
+      if (fuse.dvec) gamma_from_dvec(p, dvec.as<double>(), gamma.as<double>(), s);
+      j_from_gamma(p, gamma.as<double>(), J, s);
+      p.timer.mark(kPhJ, s);
+      return;
     }
     gamma_from_dvec(p, dvec.as<double>(), gamma.as<double>(), s);
     j_from_gamma(p, gamma.as<double>(), J, s);

@@ -236,18 +236,21 @@ def _main(argv=None):
     ap.add_argument("--lebedev", type=int, default=302)
     ap.add_argument("--repeat", type=int, default=1, help="solves (the last one is reported)")
     ap.add_argument("--guess", default="core", choices=["core", "sad"])
+    ap.add_argument("--streamed", action="store_true",
+                    help="streamed DF (B rebuilt per J/K call, not held): df(aux, chunk=...)")
     a = ap.parse_args(argv)
     sym, xyz, orb, aux, nocc = systems.workload(a.workload, seed=0)
     for _ in range(a.repeat):
         t0 = time.perf_counter()
-        ks = KS(sym, xyz, orb, coulomb=df(aux, precision=a.precision), xc=a.xc,
+        ks = KS(sym, xyz, orb, coulomb=df(aux, precision=a.precision,
+                                           chunk=1 if a.streamed else None), xc=a.xc,
                 grid=becke(a.radial, a.lebedev))
         r = scf(ks, guess=a.guess)
         sec = time.perf_counter() - t0
         ks.close()
         ks.plan.close()
     print(json.dumps({"workload": a.workload, "precision": a.precision, "xc": a.xc,
-                      "guess": a.guess,
+                      "guess": a.guess, "streamed": a.streamed,
                       "e_tot": r.e_tot, "converged": r.converged, "n_iter": r.n_iter,
                       "seconds": round(sec, 3), "parts_ms": r.timings_ms,
                       "xc_chunk": r.xc_chunk, "xc_graph": r.xc_graph}))
