@@ -81,7 +81,7 @@ def test_mixed_vs_fp64(name, ncol):
 def test_mixed_vs_fp64_benchmark_workloads(name):
     """The benchmark's own workloads (geometry seed 0, C_occ seed 100 as in
     bench.py): the mixed result against the float64 result of the same plan
-    inputs. The north star's bar is |dE| <= 1 uHa per molecule; the tighter
+    inputs. The accuracy bar of the mixed form is |dE| <= 1 uHa per molecule; the tighter
     E_ABS is what these workloads are measured to hold (1.2e-9 Ha on (H2O)_32,
     2.4e-8 Ha on C20H42)."""
     import torch
