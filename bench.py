@@ -268,20 +268,21 @@ def timed_steps(torch, step, steps, warmup, stream, barrier, lib):
     return e0.elapsed_time(e1), (lib.dfjk_kernel_launches() - l0) // max(steps, 1)
 
 
-def run_ours(args, rank, world, local_rank):
+def rank_sync(world, backend="nccl", device="cuda", local_rank=0):
+    """(barrier, max_over_ranks, dist) for a run of `world` ranks, one per GPU
+    (replicas: no collective in the measured work; the ranks only line up
+    their timed regions and take the slowest one). `backend="gloo"` with
+    `device="cpu"` serves the CPU test of this plumbing."""
+    import datetime
+
     import torch
 
-    from dftax_b200 import Plan, _lib, systems
-
-    torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
-        import datetime
-
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
-                                device_id=torch.device(f"cuda:{local_rank}"))
+        kw = {"device_id": torch.device(f"cuda:{local_rank}")} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=900), **kw)
 
     def barrier():
         if dist is not None:
@@ -290,9 +291,20 @@ def run_ours(args, rank, world, local_rank):
     def max_over_ranks(x):
         if dist is None:
             return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    return barrier, max_over_ranks, dist
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from dftax_b200 import Plan, _lib, systems
+
+    torch.cuda.set_device(local_rank)
+    barrier, max_over_ranks, dist = rank_sync(world, local_rank=local_rank)
 
     head = "mixed" if args.precision in ("both", "mixed") else "fp64"
     precs = [head] + (["fp64"] if args.precision == "both" else [])
