@@ -79,7 +79,7 @@ class ScfOptions(ctypes.Structure):
                 ("level_shift", c_double), ("rho_thresh", c_double), ("ao_thresh", c_double),
                 ("max_iter", c_int32),
                 ("diis_space", c_int32), ("grid_chunk", c_int64), ("xc_streams", c_int32),
-                ("reserved", c_int32)]
+                ("density", c_int32)]
 
 
 class ScfResult(ctypes.Structure):
@@ -88,7 +88,7 @@ class ScfResult(ctypes.Structure):
                 ("n_iter", c_int32), ("converged", c_int32), ("nmo", c_int32),
                 ("nocc", c_int32), ("ms_jk", c_double), ("ms_xc", c_double),
                 ("ms_diag", c_double), ("ms_diis", c_double), ("xc_chunk", c_int64),
-                ("xc_graph", c_int32), ("reserved", c_int32)]
+                ("xc_graph", c_int32), ("n_eig", c_int32)]
 
 
 class BatchOptions(ctypes.Structure):

@@ -111,7 +111,7 @@ int64_t estimate(const dfbatch_request* r) {
   const int64_t x = std::min<int64_t>((int64_t)6 << 30, nao * ldb * nocc * 8);
   b += x + x * 5 / 8 + (ldb * nocc / 8192 + 2) * nao * nao * 8;  // K half transform, slices, partials
   const int64_t diis = r->scf_opts.diis_space > 0 ? r->scf_opts.diis_space : 8;
-  b += (14 + 2 * diis) * nao * nao * 8;                          // SCF matrices, DIIS
+  b += (18 + 2 * diis) * nao * nao * 8;                          // SCF matrices (purification too), DIIS
   const int64_t G = r->scf_opts.grid_chunk > 0 ? r->scf_opts.grid_chunk : 16384;
   // XC chunk buffers and a V accumulator on each of the solve's XC streams
   // (one unless the request asks for more: xc.cu), the grid

@@ -13,7 +13,10 @@
 //   on the filled ones (scf.py:245-273), solved on the host;
 //   optional level shift b (S - S P S / 2) (scf.py:367);
 //   X^T F X diagonalized in float64 (cuSOLVER syevd), C = X C', P_{k+1} =
-//   2 C_occ C_occ^T (scf.py:319-327);
+//   2 C_occ C_occ^T (scf.py:319-327); or, with the purification option, the
+//   same aufbau projector of X^T F X by SP2 iterations (GEMMs), C_occ from a
+//   projected Cholesky QR, and the eigensolver once at the end for the
+//   orbitals and their energies;
 //   E(P_{k+1}) and F(P_{k+1}) together; converged when |E_{k+1} - E_k| < e_tol
 //   and |err_k| < d_tol (scf.py:371).
 // X is the canonical orthonormalizer U s^-1/2 over the overlap eigenvalues
@@ -47,10 +50,15 @@ struct dfscf {
   dfjk::DevBuf S, T, V, H, X;
   dfjk::DevBuf P, C, eps, F, J, K, Vxc, Cocc, wocc;
   dfjk::DevBuf dF, dE, A1, A2, Fo, work, info, vec;
+  dfjk::DevBuf Fx;                                   // the DIIS Fock matrix of the iteration
+  dfjk::DevBuf sp_X, sp_X2, sp_Z, sp_Y, sp_Q, sp_st, sp_info, sp_work;   // purification
+  bool sp_have_Q = false;      // sp_Q holds the last occupied orbitals (X^T-basis)
+  int sp_steps = 16;           // projection steps the last converged density took
   dfjk::XcWork xcw;
   std::vector<double> B;   // DIIS error overlaps, m x m
   dfscf_result res{};
   bool have_orbitals = false;
+  bool orbitals_current = false;   // C / eps diagonalize the Fock matrix of the last density
   int64_t tuned_chunk = 0;   // XC points per chunk chosen by the autotuner (0: not tuned)
 };
 
@@ -95,6 +103,111 @@ __global__ void antisym_kernel(const double* __restrict__ Bm, int n, double* __r
 }
 
 unsigned blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+// --- density by purification (SP2) -----------------------------------------
+// Second-order spectral projection (A. M. N. Niklasson, Phys. Rev. B 66,
+// 155115 (2002)), trace-correcting form: X_0 maps the spectrum of the
+// orthonormal-basis Fock matrix A into [0, 1] with the lowest eigenvalues
+// nearest 1; each step applies x^2 or 2x - x^2, whichever brings the trace
+// nearer nocc. With a gap between the nocc-th and the next eigenvalue the
+// eigenvalues go to 1 (occupied) and 0 (virtual): X is then the aufbau
+// projector C'_occ C'_occ^T that the eigensolver path builds.
+
+// Gershgorin bounds of the symmetric m x m matrix A (column-major):
+// out[0] <= every eigenvalue <= out[1]. One block; thread r sums rows r,
+// r + 1024, ... (a warp reads 32 consecutive rows of one column at a time).
+__global__ void __launch_bounds__(1024) gershgorin_kernel(const double* __restrict__ A, int m,
+                                                          double* __restrict__ out) {
+  __shared__ double slo[1024], shi[1024];
+  double lo = INFINITY, hi = -INFINITY;
+  for (int r = threadIdx.x; r < m; r += 1024) {
+    double off = 0.0;
+    for (int c = 0; c < m; ++c)
+      if (c != r) off += fabs(A[(int64_t)c * m + r]);
+    const double d = A[(int64_t)r * m + r];
+    lo = fmin(lo, d - off);
+    hi = fmax(hi, d + off);
+  }
+  slo[threadIdx.x] = lo;
+  shi[threadIdx.x] = hi;
+  __syncthreads();
+  for (int w = 512; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      slo[threadIdx.x] = fmin(slo[threadIdx.x], slo[threadIdx.x + w]);
+      shi[threadIdx.x] = fmax(shi[threadIdx.x], shi[threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = slo[0];
+    out[1] = shi[0];
+  }
+}
+
+// X_0 = (hi I - A) / (hi - lo) with b = {lo, hi} (zero when hi = lo, which
+// then fails the trace test and falls back to the eigensolver)
+__global__ void sp2_init_kernel(const double* __restrict__ A, int m, const double* __restrict__ b,
+                                double* __restrict__ X) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)m * m) return;
+  const int64_t r = i % m, c = i / m;
+  const double w = b[1] - b[0];
+  X[i] = w > 0.0 ? ((r == c ? b[1] : 0.0) - A[i]) / w : 0.0;
+}
+
+// One projection step from X (in) and Z = X X to Xn (out; a separate
+// buffer, since every block first reads the diagonals of X and Z): the
+// traces t1 = Tr X and t2 = Tr Z, reduced by every block in the same fixed
+// order so all take the same branch, then Xn = sym(Z) when Tr X^2 is nearer
+// nocc than Tr(2X - X^2), else 2X - sym(Z). Block 0 records {t1, t2, branch}.
+constexpr int kSp2Threads = 512;
+__global__ void __launch_bounds__(kSp2Threads) sp2_step_kernel(const double* __restrict__ X,
+                                                              const double* __restrict__ Z, int m,
+                                                              int nocc, double* __restrict__ Xn,
+                                                              double* __restrict__ rec) {
+  __shared__ double s1[kSp2Threads], s2[kSp2Threads];
+  double a = 0.0, b = 0.0;
+  for (int r = threadIdx.x; r < m; r += kSp2Threads) {
+    a += X[(int64_t)r * m + r];
+    b += Z[(int64_t)r * m + r];
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = kSp2Threads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  const double t1 = s1[0], t2 = s2[0], N = (double)nocc;
+  const bool sq = fabs(t2 - N) < fabs(2.0 * t1 - t2 - N);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    rec[0] = t1;
+    rec[1] = t2;
+    rec[2] = sq ? 1.0 : 0.0;
+  }
+  const int64_t mm = (int64_t)m * m;
+  for (int64_t i = blockIdx.x * (int64_t)kSp2Threads + threadIdx.x; i < mm;
+       i += (int64_t)gridDim.x * kSp2Threads) {
+    const int64_t r = i % m, c = i / m;
+    const double z = 0.5 * (Z[i] + Z[c + r * (int64_t)m]);
+    Xn[i] = sq ? z : 2.0 * X[i] - z;
+  }
+}
+
+// deterministic start vectors in [-1, 1): splitmix64 (Steele, Lea and Flood,
+// OOPSLA 2014) of the element index
+__global__ void fill_hash_kernel(double* __restrict__ R, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = (uint64_t)i + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  R[i] = (double)(z >> 11) * 0x1.0p-52 - 1.0;
+}
 
 // adds the milliseconds of the device work enqueued on s since the last mark
 struct PartTimer {
@@ -200,8 +313,8 @@ double energy_fock(dfscf& f, const double* P, bool from_orbitals, double* Fout, 
   return e_one + e_coul + e_xc + f.e_nn;
 }
 
-// orbitals of F into f.C / f.eps and the aufbau density into f.P
-void make_density(dfscf& f, const double* Fm, cudaStream_t s) {
+// orbitals of F into f.C / f.eps and (write_P) the aufbau density into f.P
+void make_density_eig(dfscf& f, const double* Fm, cudaStream_t s, bool write_P = true) {
   Context& c = *f.c;
   PartTimer tm(s);
   const int n = f.nao, m = f.nmo;
@@ -214,15 +327,148 @@ void make_density(dfscf& f, const double* Fm, cudaStream_t s) {
   // C = X C'
   gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, 1.0, f.X.as<double>(), n, f.Fo.as<double>(), m, 0.0,
        f.C.as<double>(), n, s);
-  // P = 2 C_occ C_occ^T (lower by SYRK, then mirrored)
-  const double two = 2.0, zero = 0.0;
+  if (write_P) {
+    // P = 2 C_occ C_occ^T (lower by SYRK, then mirrored)
+    const double two = 2.0, zero = 0.0;
+    DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+    DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, f.nocc, &two,
+                            f.C.as<double>(), n, &zero, f.P.as<double>(), n));
+    fill_upper_kernel<<<blocks((int64_t)n * n), 256, 0, s>>>(f.P.as<double>(), n);
+    DFJK_LAUNCHED();
+    ++f.res.n_eig;
+  }
+  tm.add(f.res.ms_diag);
+  f.have_orbitals = true;
+  f.orbitals_current = true;
+}
+
+constexpr int kSp2Max = 96;     // projection steps before giving up (no gap)
+
+// The aufbau density of F by SP2 purification into f.P, with C_occ (only
+// the occupied columns of f.C). Returns false, with f.P untouched, when the
+// projection does not converge to a rank-nocc projector.
+bool sp2_density(dfscf& f, const double* Fm, cudaStream_t s) {
+  Context& c = *f.c;
+  PartTimer tm(s);
+  const int n = f.nao, m = f.nmo, k = f.nocc;
+  const int64_t mm = (int64_t)m * m;
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, m, n, 1.0, Fm, n, f.X.as<double>(), n, 0.0, f.A1.as<double>(),
+       n, s);
+  gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, 1.0, f.X.as<double>(), n, f.A1.as<double>(), n, 0.0,
+       f.Fo.as<double>(), m, s);
+  double* Xb[2] = {f.sp_X.as<double>(), f.sp_X2.as<double>()};
+  double* Z = f.sp_Z.as<double>();
+  double* st = f.sp_st.as<double>();   // [0..1] bounds, then 3 per step
+  gershgorin_kernel<<<1, 1024, 0, s>>>(f.Fo.as<double>(), m, st);
+  DFJK_LAUNCHED();
+  sp2_init_kernel<<<blocks(mm), 256, 0, s>>>(f.Fo.as<double>(), m, st, Xb[0]);
+  DFJK_LAUNCHED();
+  const unsigned grid =
+      (unsigned)std::min<int64_t>((mm + 4 * kSp2Threads - 1) / (4 * kSp2Threads), 4 * 148);
+  // Stop on the idempotency error e = Tr X - Tr X^2 = sum l (1 - l): below
+  // m 1e-15, or once it is below 1e-9 and no longer falling (the rounding
+  // floor; steps enqueued after that point keep X at the floor). The first
+  // host check comes after as many steps as the last converged projection
+  // took (the spectra of consecutive iterations are alike), then every 4.
+  std::vector<double> hs(3 * kSp2Max);
+  double e1 = INFINITY, e2 = INFINITY, t1_last = 0.0;
+  bool done = false;
+  int it = 0, cur = 0;
+  while (it < kSp2Max && !done) {
+    const int g = std::min(it == 0 ? std::max(f.sp_steps, 4) : 4, kSp2Max - it);
+    for (int j = 0; j < g; ++j) {
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, 1.0, Xb[cur], m, Xb[cur], m, 0.0, Z, m, s);
+      sp2_step_kernel<<<grid, kSp2Threads, 0, s>>>(Xb[cur], Z, m, k, Xb[cur ^ 1],
+                                                   st + 2 + 3 * (it + j));
+      DFJK_LAUNCHED();
+      cur ^= 1;
+    }
+    DFJK_CUDA(cudaMemcpyAsync(hs.data(), st + 2 + 3 * it, 3 * g * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    DFJK_CUDA(cudaStreamSynchronize(s));
+    bool bad = false;
+    for (int j = 0; j < g && !done; ++j) {
+      const double e = std::fabs(hs[3 * j] - hs[3 * j + 1]);
+      t1_last = hs[3 * j];
+      if (!std::isfinite(e)) {
+        bad = true;
+        break;
+      }
+      if (e < 1e-15 * m || (e < 1e-9 && e >= e2)) {
+        done = true;
+        f.sp_steps = it + j + 1;
+      }
+      e2 = e1;
+      e1 = e;
+    }
+    if (bad) break;
+    it += g;
+  }
+  const double* Xs = Xb[cur];
+  if (!done || !(std::fabs(t1_last - k) < 1e-6)) {
+    tm.add(f.res.ms_diag);
+    return false;
+  }
+  // C'_occ: X applied to the last occupied orbitals (or to fixed
+  // pseudo-random vectors), orthonormalized by Cholesky QR, twice; the second
+  // pass projects out what the first left outside range(X)
+  double* Y = f.sp_Y.as<double>();
+  double* Q = f.sp_Q.as<double>();
+  double* M = f.A2.as<double>();   // k x k
+  const int64_t mk = (int64_t)m * k;
+  if (!f.sp_have_Q) {
+    fill_hash_kernel<<<blocks(mk), 256, 0, s>>>(Q, mk);
+    DFJK_LAUNCHED();
+  }
+  f.sp_have_Q = false;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  DFJK_CUSOLVER(cusolverDnSetStream(c.cusolver, s));
+  int lwork = 0;
+  DFJK_CUSOLVER(cusolverDnDpotrf_bufferSize(c.cusolver, CUBLAS_FILL_MODE_LOWER, k, M, k, &lwork));
+  f.sp_work.ensure((size_t)std::max(lwork, 1) * sizeof(double));
+  for (int pass = 0; pass < 2; ++pass) {
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, m, k, m, 1.0, Xs, m, Q, m, 0.0, Y, m, s);
+    DFJK_CUBLAS(cublasSetStream(c.cublas, s));
+    DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, k, m, &one, Y, m, &zero,
+                            M, k));
+    DFJK_CUSOLVER(cusolverDnDpotrf(c.cusolver, CUBLAS_FILL_MODE_LOWER, k, M, k,
+                                   f.sp_work.as<double>(), lwork, f.sp_info.as<int>() + pass));
+    // Y <- Y L^-T, then Q = Y
+    DFJK_CUBLAS(cublasDtrsm(c.cublas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                            CUBLAS_DIAG_NON_UNIT, m, k, &one, M, k, Y, m));
+    DFJK_CUDA(cudaMemcpyAsync(Q, Y, mk * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  }
+  // |X Q - Q|_F: Q must lie in range(X)
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, m, k, m, 1.0, Xs, m, Q, m, 0.0, Y, m, s);
+  DFJK_CUBLAS(cublasDaxpy(c.cublas, (int)mk, &mone, Q, 1, Y, 1));
+  double res = 0.0;
+  DFJK_CUBLAS(cublasDnrm2(c.cublas, (int)mk, Y, 1, &res));
+  int hinfo[2] = {0, 0};
+  DFJK_CUDA(cudaMemcpyAsync(hinfo, f.sp_info.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFJK_CUDA(cudaStreamSynchronize(s));
+  if (hinfo[0] != 0 || hinfo[1] != 0 || !(res < 1e-10 * std::sqrt((double)k))) {
+    tm.add(f.res.ms_diag);
+    return false;
+  }
+  f.sp_have_Q = true;
+  // C_occ = X C'_occ (first k columns of f.C), P = 2 C_occ C_occ^T
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, 1.0, f.X.as<double>(), n, Q, m, 0.0, f.C.as<double>(),
+       n, s);
+  const double two = 2.0;
   DFJK_CUBLAS(cublasSetStream(c.cublas, s));
-  DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, f.nocc, &two,
+  DFJK_CUBLAS(cublasDsyrk(c.cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, k, &two,
                           f.C.as<double>(), n, &zero, f.P.as<double>(), n));
   fill_upper_kernel<<<blocks((int64_t)n * n), 256, 0, s>>>(f.P.as<double>(), n);
   DFJK_LAUNCHED();
   tm.add(f.res.ms_diag);
-  f.have_orbitals = true;
+  f.orbitals_current = false;
+  return true;
+}
+
+// the aufbau density of F into f.P with C_occ in f.C, by the configured route
+void make_density(dfscf& f, const double* Fm, cudaStream_t s) {
+  if (f.o.density == 1 && f.nocc < f.nmo && sp2_density(f, Fm, s)) return;
+  make_density_eig(f, Fm, s);
 }
 
 // err = X^T (F P S - S P F) X into f.Fo's slot of dE; returns |err|
@@ -300,7 +546,7 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
     DFJK_CUDA(cudaMemcpyAsync(f.P.p, P0, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
     orbitals = false;
   } else {
-    make_density(f, f.H.as<double>(), s);   // core-Hamiltonian guess
+    make_density_eig(f, f.H.as<double>(), s);   // core-Hamiltonian guess
     orbitals = true;
   }
   double e_prev = energy_fock(f, f.P.as<double>(), orbitals, f.F.as<double>(), s);
@@ -347,15 +593,18 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
       const double b = f.o.level_shift;
       DFJK_CUBLAS(cublasDaxpy(c.cublas, (int)nn, &b, f.S.as<double>(), 1, Fext, 1));
     }
-    // the DIIS Fock moves to the dedicated buffer before make_density reuses A1/A2
-    DFJK_CUDA(cudaMemcpyAsync(f.Vxc.p, Fext, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    // the DIIS Fock moves to its own buffer before make_density reuses A1/A2
+    DFJK_CUDA(cudaMemcpyAsync(f.Fx.p, Fext, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
     tm.add(f.res.ms_diis);
-    make_density(f, f.Vxc.as<double>(), s);
+    make_density(f, f.Fx.as<double>(), s);
     const double e = energy_fock(f, f.P.as<double>(), true, f.F.as<double>(), s);
     converged = std::fabs(e - e_prev) < f.o.e_tol && derr < f.o.d_tol;
     e_prev = e;
     ++it;
   }
+  // orbitals and energies of the last DIIS Fock matrix when the density came
+  // from the projection (the density itself stays)
+  if (it > 0 && !f.orbitals_current) make_density_eig(f, f.Fx.as<double>(), s, false);
   f.res.e_tot = e_prev;
   f.res.derr = derr;
   f.res.xc_chunk = f.xcw.ch.G;
@@ -389,7 +638,7 @@ void autotune_chunk(dfscf& f, const int (&nout)[8], const std::vector<double>& p
     if (it != tuned().end()) best = it->second;
   }
   if (best == 0) {
-    make_density(f, f.H.as<double>(), s);   // core-guess density to time on
+    make_density_eig(f, f.H.as<double>(), s);   // core-guess density to time on
     double best_ms = INFINITY;
     f.xcw.graph_off = true;
     for (int64_t G : {4096, 8192, 16384}) {
@@ -438,6 +687,7 @@ void dfscf_default_options(dfscf_options* o) {
   o->diis_space = 8;
   o->grid_chunk = 0;
   o->xc_streams = 0;
+  o->density = 1;
 }
 
 dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
@@ -465,6 +715,7 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     if (f->o.xc_streams < 0 || f->o.xc_streams > kXcBranches)
       fail(DFJK_ERR_INVALID, "xc_streams must be 0..%d", kXcBranches);
     f->xcw.nbr = f->o.xc_streams > 0 ? f->o.xc_streams : kXcBranches;
+    if (f->o.density != 0 && f->o.density != 1) fail(DFJK_ERR_INVALID, "density must be 0 or 1");
     for (int64_t i = 0; i < 3 * (int64_t)natom; ++i)
       if (!std::isfinite(atom_xyz[i])) fail(DFJK_ERR_NUMERIC, "non-finite atom coordinate");
     for (int64_t i = 0; i < 3 * npoint; ++i)
@@ -545,6 +796,16 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     f->eps.alloc(m * sizeof(double));
     f->Fo.alloc(m * m * sizeof(double));
     f->Cocc.alloc(n * nocc * sizeof(double));
+    f->Fx.alloc(nn * sizeof(double));
+    if (f->o.density == 1) {
+      f->sp_X.alloc(m * m * sizeof(double));
+      f->sp_X2.alloc(m * m * sizeof(double));
+      f->sp_Z.alloc(m * m * sizeof(double));
+      f->sp_Y.alloc(m * nocc * sizeof(double));
+      f->sp_Q.alloc(m * nocc * sizeof(double));
+      f->sp_st.alloc((2 + 3 * kSp2Max) * sizeof(double));
+      f->sp_info.alloc(2 * sizeof(int));
+    }
     upload(f->wocc, std::vector<double>(nocc, 2.0));
     f->dF.alloc((size_t)f->o.diis_space * nn * sizeof(double));
     f->dE.alloc((size_t)f->o.diis_space * m * m * sizeof(double));

@@ -53,6 +53,10 @@ class KSResult:
     timings_ms: dict | None = None   # J/K, XC, diagonalization, DIIS of the run
     xc_chunk: int = 0                # grid points per XC chunk (set or autotuned)
     xc_graph: bool = False           # XC evaluations replayed a captured CUDA graph
+    n_eig: int = 0                   # densities built by the eigensolver (guess, fallbacks)
+
+
+DENSITY_ROUTES = {"eigh": 0, "purify": 1}
 
 
 class KS:
@@ -61,9 +65,14 @@ class KS:
     def __init__(self, symbols, coords_bohr, basis: BasisData, *, coulomb: DFSpec, xc="PBE0",
                  grid=None, charges=None, device: int = 0, diis_space: int = 8,
                  lindep_thresh: float = 1e-7, plan: Plan | None = None,
-                 ao_thresh: float = 1e-14, grid_chunk: int = 0, xc_streams: int = 0):
+                 ao_thresh: float = 1e-14, grid_chunk: int = 0, xc_streams: int = 0,
+                 density: str = "purify"):
         if xc not in XC_FUNCTIONALS:
             raise ValueError(f"xc must be one of {sorted(XC_FUNCTIONALS)}")
+        # each iteration's aufbau density: "purify" (SP2 projection, the
+        # eigensolver when it does not converge) or "eigh" (the eigensolver)
+        if density not in DENSITY_ROUTES:
+            raise ValueError(f"density must be one of {sorted(DENSITY_ROUTES)}")
         if not isinstance(coulomb, DFSpec) or not isinstance(coulomb.auxbasis, BasisData):
             raise TypeError("coulomb must be df(aux) with a built auxiliary BasisData")
         self.torch = _torch()
@@ -98,6 +107,7 @@ class KS:
         self._diis, self._lindep = diis_space, lindep_thresh
         self._ao_thresh, self._grid_chunk = float(ao_thresh), int(grid_chunk)
         self._xc_streams = int(xc_streams)   # 0: 8 concurrent XC streams; the batch engine uses 1
+        self._density = DENSITY_ROUTES[density]
         self.h = ctypes.c_void_p()
         self._create()
 
@@ -113,6 +123,7 @@ class KS:
         o.ao_thresh = self._ao_thresh
         o.grid_chunk = self._grid_chunk
         o.xc_streams = self._xc_streams
+        o.density = self._density
         self._opts = o
         _lib.check(self.lib.dfscf_create(self.plan.h, len(self.charges), self.coords.ctypes.data,
                                          self.charges.ctypes.data, len(self.grid_weights),
@@ -212,10 +223,10 @@ def scf(ks: KS, *, max_iter: int = 128, e_tol: float = 1e-8, d_tol: float = 1e-6
                     e_coul=r.e_coul,
                     timings_ms={"jk": r.ms_jk, "xc": r.ms_xc, "diag": r.ms_diag,
                                 "diis": r.ms_diis},
-                    xc_chunk=int(r.xc_chunk), xc_graph=bool(r.xc_graph))
+                    xc_chunk=int(r.xc_chunk), xc_graph=bool(r.xc_graph), n_eig=int(r.n_eig))
 
 
-__all__ = ["KS", "KSResult", "scf", "XC_FUNCTIONALS"]
+__all__ = ["KS", "KSResult", "scf", "XC_FUNCTIONALS", "DENSITY_ROUTES"]
 
 
 def _main(argv=None):
@@ -236,6 +247,7 @@ def _main(argv=None):
     ap.add_argument("--lebedev", type=int, default=302)
     ap.add_argument("--repeat", type=int, default=1, help="solves (the last one is reported)")
     ap.add_argument("--guess", default="core", choices=["core", "sad"])
+    ap.add_argument("--density", default="purify", choices=sorted(DENSITY_ROUTES))
     ap.add_argument("--streamed", action="store_true",
                     help="streamed DF (B rebuilt per J/K call, not held): df(aux, chunk=...)")
     a = ap.parse_args(argv)
@@ -244,16 +256,16 @@ def _main(argv=None):
         t0 = time.perf_counter()
         ks = KS(sym, xyz, orb, coulomb=df(aux, precision=a.precision,
                                            chunk=1 if a.streamed else None), xc=a.xc,
-                grid=becke(a.radial, a.lebedev))
+                grid=becke(a.radial, a.lebedev), density=a.density)
         r = scf(ks, guess=a.guess)
         sec = time.perf_counter() - t0
         ks.close()
         ks.plan.close()
     print(json.dumps({"workload": a.workload, "precision": a.precision, "xc": a.xc,
-                      "guess": a.guess, "streamed": a.streamed,
+                      "guess": a.guess, "density": a.density, "streamed": a.streamed,
                       "e_tot": r.e_tot, "converged": r.converged, "n_iter": r.n_iter,
                       "seconds": round(sec, 3), "parts_ms": r.timings_ms,
-                      "xc_chunk": r.xc_chunk, "xc_graph": r.xc_graph}))
+                      "xc_chunk": r.xc_chunk, "xc_graph": r.xc_graph, "n_eig": r.n_eig}))
 
 
 if __name__ == "__main__":

@@ -47,7 +47,14 @@ typedef struct {
   int32_t xc_streams;   /* concurrent streams the XC chunks run on, 1..8 (0: 8); the
                            batch engine runs its solves, which already overlap one
                            another, with 1                                             */
-  int32_t reserved;
+  int32_t density;      /* how each iteration's density comes from the DIIS Fock matrix:
+                           0: its eigenvectors (cuSOLVER syevd) and aufbau occupations;
+                           1: second-order spectral projection (SP2 purification) of
+                           X^T F X onto its nocc lowest eigenvalues, which is the same
+                           aufbau density when the HOMO-LUMO gap is open, falling back
+                           to the eigensolver for that iteration when the projection
+                           does not converge (no gap). The orbitals and energies of
+                           dfscf_get_orbitals come from the eigensolver either way  */
 } dfscf_options;
 
 typedef struct {
@@ -67,7 +74,9 @@ typedef struct {
   double ms_jk, ms_xc, ms_diag, ms_diis;
   int64_t xc_chunk;     /* grid points per XC chunk (set, or chosen by the autotuner)    */
   int32_t xc_graph;     /* 1: the XC evaluations replayed a captured CUDA graph          */
-  int32_t reserved;
+  int32_t n_eig;        /* densities built by the eigensolver in the last dfscf_run: the
+                           core guess and every iteration with density 0; the core
+                           guess and the fallbacks with density 1                       */
 } dfscf_result;
 
 /* dftax's defaults for PBE0 (scf.py:279-391, xc.py:584-601, grid.py:10-45). */

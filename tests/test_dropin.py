@@ -63,6 +63,16 @@ def test_range_separated_needs_omega(water_golden):
         B200DFCoulomb(golden_basis(g, "orb"), golden_basis(g, "aux"), 0.2, hf_coeff_lr=0.8)
 
 
+def test_ks_rejects_an_unknown_density_route(water_golden):
+    """Checked before any device work."""
+    from dftax_b200 import df
+    from dftax_b200.ks import KS
+
+    orb, aux = golden_basis(water_golden, "orb"), golden_basis(water_golden, "aux")
+    with pytest.raises(ValueError, match="density must be one of"):
+        KS(["O", "H", "H"], np.zeros((3, 3)), orb, coulomb=df(aux), density="diagonalize")
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision,tol", [("fp64", NOISE_REL), ("mixed", 1e-7)])
 def test_make_coulomb_energy_and_fock_vs_reference(water_golden, precision, tol):
