@@ -615,7 +615,7 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
 
 // Points per XC chunk, chosen by timing: the chunk size sets the shapes of the
 // two DGEMMs per chunk (G x nsig x nsig) and the launches per evaluation.
-// Candidates 4096, 8192 and 16384 points are timed on the core-guess density
+// Candidates 2048, 4096, 8192 and 16384 points are timed on the core-guess density
 // (two evaluations each, the second timed, launched directly) for the first
 // molecule of each (nao / 128, log2 points) bucket; the choice is kept for
 // the process, so later molecules of that size (solves in a batch included)
@@ -641,7 +641,7 @@ void autotune_chunk(dfscf& f, const int (&nout)[8], const std::vector<double>& p
     make_density_eig(f, f.H.as<double>(), s);   // core-guess density to time on
     double best_ms = INFINITY;
     f.xcw.graph_off = true;
-    for (int64_t G : {4096, 8192, 16384}) {
+    for (int64_t G : {2048, 4096, 8192, 16384}) {
       if ((int64_t)6 * f.nao * G * 8 > ((int64_t)3 << 30)) continue;
       xc_chunk(f.p->orb, nout, pv, G, f.o.ao_thresh, f.xcw);
       xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),

@@ -42,7 +42,7 @@ typedef struct {
   int32_t max_iter;     /* 128                                                          */
   int32_t diis_space;   /* DIIS history depth (8)                                        */
   int64_t grid_chunk;   /* grid points per XC chunk, spatially sorted (0: chosen by
-                           timing 4096, 8192 and 16384 on the first molecule of each
+                           timing 2048, 4096, 8192 and 16384 on the first molecule of each
                            size; the choice is kept for the process)                   */
   int32_t xc_streams;   /* concurrent streams the XC chunks run on, 1..8 (0: 8); the
                            batch engine runs its solves, which already overlap one
