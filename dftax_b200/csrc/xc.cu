@@ -473,19 +473,28 @@ void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
     code[i] = morton3(c[0], c[1], c[2]);
     cmax = std::max(cmax, code[i]);
   }
-  // order by (code, index): a stable counting sort over the codes when they
-  // are few (a molecule spans a few dozen cells per axis), else a sort
-  std::vector<int64_t> order(n);
-  if (cmax < ((uint64_t)1 << 24)) {
-    std::vector<int64_t> start(cmax + 2, 0);
-    for (int64_t i = 0; i < n; ++i) start[code[i] + 1]++;
-    for (uint64_t k = 0; k <= cmax; ++k) start[k + 1] += start[k];
-    for (int64_t i = 0; i < n; ++i) order[start[code[i]]++] = i;
-  } else {
-    std::vector<std::pair<uint64_t, int64_t>> key(n);
-    for (int64_t i = 0; i < n; ++i) key[i] = {code[i], i};
-    std::sort(key.begin(), key.end());
-    for (int64_t i = 0; i < n; ++i) order[i] = key[i].second;
+  // order by (code, index): a stable LSD radix sort of the codes, 11 bits
+  // a pass over the bits cmax needs (the outermost radial points lie
+  // thousands of Bohr out, so the codes span tens of bits)
+  int bits = 0;
+  while (bits < 64 && (cmax >> bits) != 0) ++bits;
+  constexpr int kRadixBits = 11;
+  constexpr uint64_t kMask = ((uint64_t)1 << kRadixBits) - 1;
+  std::vector<int64_t> order(n), otmp(n);
+  std::vector<uint64_t> ktmp(n);
+  for (int64_t i = 0; i < n; ++i) order[i] = i;
+  std::vector<int64_t> cnt(kMask + 2);
+  for (int shift = 0; shift < bits; shift += kRadixBits) {
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (int64_t i = 0; i < n; ++i) cnt[((code[i] >> shift) & kMask) + 1]++;
+    for (uint64_t k = 0; k <= kMask; ++k) cnt[k + 1] += cnt[k];
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t dst = cnt[(code[i] >> shift) & kMask]++;
+      ktmp[dst] = code[i];
+      otmp[dst] = order[i];
+    }
+    code.swap(ktmp);
+    order.swap(otmp);
   }
   std::vector<double> p2(3 * n), w2(n);
   for (int64_t i = 0; i < n; ++i) {
