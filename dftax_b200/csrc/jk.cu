@@ -105,12 +105,26 @@ __global__ void j_rows_kernel(const double* __restrict__ B, int64_t ldb, int64_t
   const int64_t nwarps = (gridDim.x * (int64_t)blockDim.x) >> 5;
   for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < nrows; r += nwarps) {
     const double* row = B + r * ldb;
-    double s = 0.0;
-    for (int64_t c = 2 * lane; c < ldb; c += 64) {
+    // four 16-byte loads in flight per lane (ldb is a multiple of 8 and c is
+    // even, so c + 192 < ldb keeps all four pairs inside the row)
+    double s4[4] = {0.0, 0.0, 0.0, 0.0};
+    int64_t c = 2 * lane;
+    for (; c + 192 < ldb; c += 256) {
+      double2 b[4], g[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        b[u] = __ldcs(reinterpret_cast<const double2*>(row + c + 64 * u));
+        g[u] = __ldg(reinterpret_cast<const double2*>(gamma + c + 64 * u));
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) s4[u] += b[u].x * g[u].x + b[u].y * g[u].y;
+    }
+    for (; c < ldb; c += 64) {
       const double2 b = __ldcs(reinterpret_cast<const double2*>(row + c));
       const double2 g = __ldg(reinterpret_cast<const double2*>(gamma + c));
-      s += b.x * g.x + b.y * g.y;
+      s4[0] += b.x * g.x + b.y * g.y;
     }
+    double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) {
