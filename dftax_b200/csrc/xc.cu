@@ -259,12 +259,13 @@ __device__ __forceinline__ D4 operator*(D4 a, D4 b) {
   for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
   return r;
 }
+// quotient rule as (a' - (a/b) b') / b: one division
 __device__ __forceinline__ D4 operator/(D4 a, D4 b) {
   D4 r;
-  r.v = a.v / b.v;
-  const double ib2 = 1.0 / (b.v * b.v);
+  const double ib = 1.0 / b.v;
+  r.v = a.v * ib;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) r.d[k] = (a.d[k] * b.v - a.v * b.d[k]) * ib2;
+  for (int k = 0; k < 4; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * ib;
   return r;
 }
 __device__ __forceinline__ D4 operator+(D4 a, double c) { a.v += c; return a; }
@@ -285,13 +286,16 @@ __device__ __forceinline__ D4 dscale(D4 a, double f) {   // chain rule with df/d
   return r;
 }
 __device__ __forceinline__ D4 dsqrt(D4 a) {
-  D4 r = dscale(a, 0.5 / sqrt(a.v));
-  r.v = sqrt(a.v);
+  const double q = sqrt(a.v);
+  D4 r = dscale(a, 0.5 / q);
+  r.v = q;
   return r;
 }
-__device__ __forceinline__ D4 dpow(D4 a, double e) {
-  D4 r = dscale(a, e * pow(a.v, e - 1.0));
-  r.v = pow(a.v, e);
+// a^(1/3) for a > 0, with d/da = a^(1/3) / (3 a)
+__device__ __forceinline__ D4 dcbrt(D4 a) {
+  const double q = cbrt(a.v);
+  D4 r = dscale(a, q / (3.0 * a.v));
+  r.v = q;
   return r;
 }
 __device__ __forceinline__ D4 dlog1p(D4 a) {
@@ -300,8 +304,9 @@ __device__ __forceinline__ D4 dlog1p(D4 a) {
   return r;
 }
 __device__ __forceinline__ D4 dexpm1(D4 a) {
-  D4 r = dscale(a, exp(a.v));
-  r.v = expm1(a.v);
+  const double q = expm1(a.v);
+  D4 r = dscale(a, a.v > -0.5 ? q + 1.0 : exp(a.v));   // e^a = expm1(a) + 1 without cancellation
+  r.v = q;
   return r;
 }
 // jnp.clip(x, lo): the bound itself (derivative 0) below lo
@@ -311,11 +316,10 @@ __device__ __forceinline__ D4 dclip(D4 a, double lo) { return a.v < lo ? dc(lo) 
 // unpolarized (xc.py: PBEExchange._unpolarized, PBECorrelation with zeta = 0)
 __device__ D4 pbe_eps(D4 rho, D4 gx, D4 gy, D4 gz, double xs, double cs) {
   constexpr double pi = 3.141592653589793;
-  constexpr double third = 1.0 / 3.0;
   // exchange
   const D4 ax = gx + 1e-30, ay = gy + 1e-30, az = gz + 1e-30;
   const D4 gnorm = dsqrt(ax * ax + ay * ay + az * az);
-  const D4 kF = dpow(3 * pi * pi * rho + 1e-30, third);
+  const D4 kF = dcbrt(3 * pi * pi * rho + 1e-30);
   const D4 s = gnorm / dclip(2 * kF * rho, 1e-30);
   const double kappa = 0.804, mu = 0.2195149727645171;
   const D4 ex_unif = -3 * kF / (4 * pi);
@@ -326,11 +330,11 @@ __device__ D4 pbe_eps(D4 rho, D4 gx, D4 gy, D4 gz, double xs, double cs) {
   const double beta = 0.06672455060314922;
   const double A = 0.0310907, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
   const D4 rt = dclip(rho, 1e-20);
-  const D4 rs = dpow(3 / (4 * pi * rt) + 1e-20, third);
+  const D4 rs = dcbrt(3 / (4 * pi * rt) + 1e-20);
   const D4 rss = dsqrt(rs);
   const D4 den = 2.0 * A * (b1 * rss + b2 * rs + b3 * rs * rss + b4 * rs * rs);
   const D4 eps_pw = -2.0 * A * (1.0 + a1 * rs) * dlog1p(1.0 / dclip(den, 1e-20));
-  const D4 kf = dpow(3 * pi * pi * rt + 1e-20, third);
+  const D4 kf = dcbrt(3 * pi * pi * rt + 1e-20);
   const D4 ks = dsqrt(4 * kf / pi);
   const D4 gn = dsqrt(gx * gx + gy * gy + gz * gz + 1e-30);
   const D4 t = gn / dclip(2 * ks * rt, 1e-20);
