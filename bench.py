@@ -556,6 +556,14 @@ def scf_measure(args, torch, precs, sym, xyz, orb, aux, world, max_over_ranks):
                      "n_iter": r.n_iter, "converged": r.converged, "e_tot_Ha": r.e_tot,
                      "iteration_parts_ms": {k: round(v, 2) for k, v in r.timings_ms.items()},
                      "xc_chunk_points": r.xc_chunk, "xc_cuda_graph": r.xc_graph,
+                     # the two float64 DGEMMs per XC chunk, over the whole XC time
+                     # (which also holds the AO, density and functional kernels)
+                     "xc_dgemm": {"tflop_per_evaluation": round(r.xc_gemm_flop / 1e12, 4),
+                                  "evaluations": r.n_iter + 1,
+                                  "tflop_s_over_xc_time": round(
+                                      r.xc_gemm_flop * (r.n_iter + 1)
+                                      / max(r.timings_ms["xc"], 1e-9) / 1e9, 2)},
+                     "eigensolver_densities": r.n_eig,
                      "setup_ms": round(1e3 * sec / args.scf_steps - it_ms, 2)}
     head = precs[0]
     line = dict(out[head])

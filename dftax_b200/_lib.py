@@ -88,7 +88,8 @@ class ScfResult(ctypes.Structure):
                 ("n_iter", c_int32), ("converged", c_int32), ("nmo", c_int32),
                 ("nocc", c_int32), ("ms_jk", c_double), ("ms_xc", c_double),
                 ("ms_diag", c_double), ("ms_diis", c_double), ("xc_chunk", c_int64),
-                ("xc_graph", c_int32), ("n_eig", c_int32)]
+                ("xc_graph", c_int32), ("n_eig", c_int32),
+                ("xc_gemm_flop", c_double)]
 
 
 class BatchOptions(ctypes.Structure):

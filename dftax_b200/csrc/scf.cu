@@ -32,6 +32,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <tuple>
 
 namespace dfjk {
 double energy(Plan& p, const double* P, int nspin, double hf, double hf_lr, double* F,
@@ -609,6 +610,7 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
   f.res.derr = derr;
   f.res.xc_chunk = f.xcw.ch.G;
   f.res.xc_graph = f.xcw.exec != nullptr ? 1 : 0;
+  f.res.xc_gemm_flop = has_xc(f) ? f.xcw.ch.gemm_flop : 0.0;
   f.res.n_iter = it;
   f.res.converged = converged ? 1 : 0;
 }
@@ -617,12 +619,12 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
 // two DGEMMs per chunk (G x nsig x nsig) and the launches per evaluation.
 // Candidates 2048, 4096, 8192 and 16384 points are timed on the core-guess density
 // (two evaluations each, the second timed, launched directly) for the first
-// molecule of each (nao / 128, log2 points) bucket; the choice is kept for
-// the process, so later molecules of that size (solves in a batch included)
-// use it without timing.
+// molecule of each (nao / 128, log2 points, XC streams) bucket; the choice is
+// kept for the process, so later molecules of that size (solves in a batch
+// included) use it without timing.
 std::mutex g_tune_mu;
-std::map<std::pair<int, int>, int64_t>& tuned() {
-  static auto* m = new std::map<std::pair<int, int>, int64_t>();
+std::map<std::tuple<int, int, int>, int64_t>& tuned() {
+  static auto* m = new std::map<std::tuple<int, int, int>, int64_t>();
   return *m;
 }
 
@@ -630,7 +632,7 @@ void autotune_chunk(dfscf& f, const int (&nout)[8], const std::vector<double>& p
                     cudaStream_t s) {
   int lg = 0;
   while ((int64_t(1) << (lg + 1)) <= f.npts) ++lg;
-  const std::pair<int, int> key{(f.nao + 127) / 128, lg};
+  const std::tuple<int, int, int> key{(f.nao + 127) / 128, lg, f.xcw.nbr};
   int64_t best = 0;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -34,6 +34,7 @@ struct XcChunks {
   std::vector<int> ao_cnt;
   int max_ao = 0;
   int64_t total_ao = 0;                // sum of ao_cnt (the dense form would be nchunk * nao)
+  double gemm_flop = 0.0;              // FLOP of one evaluation's two DGEMMs: sum 4 G ao_cnt^2
   DevBuf d_sh, d_sh_out0, d_ao_map;    // shells, their first compact AO, compact -> AO
 };
 

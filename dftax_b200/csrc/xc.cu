@@ -522,6 +522,7 @@ void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>&
   out.ao_cnt.clear();
   out.max_ao = 0;
   out.total_ao = 0;
+  out.gemm_flop = 0.0;
   out.G = G;
   if (ws.exec) cudaGraphExecDestroy(ws.exec);
   ws.exec = nullptr;
@@ -575,6 +576,7 @@ void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>&
     out.ao_cnt.push_back(nao_c);
     out.max_ao = std::max(out.max_ao, nao_c);
     out.total_ao += nao_c;
+    out.gemm_flop += 4.0 * (double)G * nao_c * nao_c;   // X = Phi P and Phi^T W
   }
   upload(out.d_sh, shl);
   upload(out.d_sh_out0, out0c);

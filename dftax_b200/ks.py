@@ -54,6 +54,7 @@ class KSResult:
     xc_chunk: int = 0                # grid points per XC chunk (set or autotuned)
     xc_graph: bool = False           # XC evaluations replayed a captured CUDA graph
     n_eig: int = 0                   # densities built by the eigensolver (guess, fallbacks)
+    xc_gemm_flop: float = 0.0        # float64 FLOP of one XC evaluation's two DGEMMs
 
 
 DENSITY_ROUTES = {"eigh": 0, "purify": 1}
@@ -223,7 +224,8 @@ def scf(ks: KS, *, max_iter: int = 128, e_tol: float = 1e-8, d_tol: float = 1e-6
                     e_coul=r.e_coul,
                     timings_ms={"jk": r.ms_jk, "xc": r.ms_xc, "diag": r.ms_diag,
                                 "diis": r.ms_diis},
-                    xc_chunk=int(r.xc_chunk), xc_graph=bool(r.xc_graph), n_eig=int(r.n_eig))
+                    xc_chunk=int(r.xc_chunk), xc_graph=bool(r.xc_graph), n_eig=int(r.n_eig),
+                    xc_gemm_flop=float(r.xc_gemm_flop))
 
 
 __all__ = ["KS", "KSResult", "scf", "XC_FUNCTIONALS", "DENSITY_ROUTES"]

@@ -43,7 +43,8 @@ typedef struct {
   int32_t diis_space;   /* DIIS history depth (8)                                        */
   int64_t grid_chunk;   /* grid points per XC chunk, spatially sorted (0: chosen by
                            timing 2048, 4096, 8192 and 16384 on the first molecule of each
-                           size; the choice is kept for the process)                   */
+                           size and XC stream count; the choice is kept for the
+                           process)                                                    */
   int32_t xc_streams;   /* concurrent streams the XC chunks run on, 1..8 (0: 8); the
                            batch engine runs its solves, which already overlap one
                            another, with 1                                             */
@@ -77,6 +78,8 @@ typedef struct {
   int32_t n_eig;        /* densities built by the eigensolver in the last dfscf_run: the
                            core guess and every iteration with density 0; the core
                            guess and the fallbacks with density 1                       */
+  double xc_gemm_flop;  /* float64 FLOP of the two DGEMMs of one XC evaluation (X = Phi P
+                           and Phi^T W per chunk: 4 G n_chunk^2 summed over the chunks) */
 } dfscf_result;
 
 /* dftax's defaults for PBE0 (scf.py:279-391, xc.py:584-601, grid.py:10-45). */
