@@ -705,6 +705,9 @@ dfjk_status dfscf_create(dfjk_plan* pl, int32_t natom, const double* atom_xyz,
     Plan& p = pl->p;
     if (!p.built) fail(DFJK_ERR_STATE, "dfscf_create before dfjk_build");
     if (p.lr) fail(DFJK_ERR_UNSUPPORTED, "the SCF does not take range-separated plans");
+    for (int l : p.orb.l)
+      if (l > kXcMaxL) fail(DFJK_ERR_UNSUPPORTED, "the SCF's AO evaluation takes l <= %d (got %d)",
+                            kXcMaxL, l);
     if (natom <= 0 || !atom_xyz || !atom_charge) fail(DFJK_ERR_INVALID, "no atoms");
     if (npoint < 0 || (npoint > 0 && (!grid_xyz || !grid_w))) fail(DFJK_ERR_INVALID, "bad grid");
     if (nocc <= 0 || nocc > p.nao) fail(DFJK_ERR_INVALID, "nocc=%d for nao=%d", nocc, p.nao);

@@ -26,10 +26,13 @@ void launch_one_electron(const Context& c, const OrbView& ov, int nshell, const 
 
 // Chunks of spatially sorted grid points, each with the orbital shells that
 // are not negligible anywhere in its bounding box (xc_prepare)
+constexpr int kXcMaxL = 3;   // orbital l the AO kernel evaluates (f)
+
 struct XcChunks {
   int64_t G = 0;                       // points per chunk (the last may hold fewer)
   std::vector<int64_t> g0, ng;         // first point and count of each chunk
   std::vector<int> sh_off, sh_cnt;     // each chunk's range in the shell list
+  std::vector<int> sh_lcnt;            // [chunk][l]: its shells of each l, in this order
   std::vector<int64_t> ao_off;         // each chunk's range in the compact AO map
   std::vector<int> ao_cnt;
   int max_ao = 0;

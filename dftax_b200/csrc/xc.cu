@@ -152,10 +152,12 @@ __device__ __forceinline__ void ao_shell(const OrbView& ov, int s, double dx, do
   }
 }
 
-// Phi[k][g] (ld G), dPhi[x][k][g] for the chunk's shells: shell j of the
-// chunk is orbital shell sh[j] with compact AOs k = out0c[j] .. ; grid
-// (ceil(G / 128), shells of the chunk); every thread of a block has the same
-// shell, so the switch on l is uniform
+// Phi[k][g] (ld G), dPhi[x][k][g] for the chunk's shells of angular momentum
+// L: shell j of the list is orbital shell shl[j] with compact AOs k =
+// out0c[j] .. ; grid (ceil(G / 128), shells of the list). One instance per L,
+// so the s and p shells, most of the work, do not carry the registers of the
+// d and f cases.
+template <int L>
 __global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const int* __restrict__ shl,
                                                         const int* __restrict__ out0c,
                                                         const double* __restrict__ pts,
@@ -166,7 +168,6 @@ __global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const int* _
   const int s = shl[blockIdx.y];
   if (g >= G) return;
   const ShellView& sh = ov.sh;
-  const int l = sh.l[s];
   const int64_t o = (int64_t)out0c[blockIdx.y] * G + g;
   const int64_t plane = (int64_t)nsig * G;
   const bool live = g < ng;
@@ -177,12 +178,7 @@ __global__ void __launch_bounds__(kAoThreads) ao_kernel(OrbView ov, const int* _
     dy = p[1] - sh.cen[3 * s + 1];
     dz = p[2] - sh.cen[3 * s + 2];
   }
-  switch (l) {
-    case 0: ao_shell<0>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
-    case 1: ao_shell<1>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
-    case 2: ao_shell<2>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
-    default: ao_shell<3>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi); break;
-  }
+  ao_shell<L>(ov, s, dx, dy, dz, live, o, G, plane, phi, dphi);
 }
 
 // Pc[k1][k2] = P[map[k1]][map[k2]]
@@ -545,6 +541,7 @@ void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>&
     return b;
   };
   std::vector<int> shl, out0c, aomap;
+  out.sh_lcnt.clear();
   for (int64_t g0 = 0; g0 < n; g0 += G) {
     const int64_t ng = std::min(G, n - g0);
     double bl[3] = {INFINITY, INFINITY, INFINITY}, bh[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -573,6 +570,28 @@ void xc_chunk(const Shells& sh, const int (&nout)[8], const std::vector<double>&
       nao_c += no;
     }
     out.sh_cnt.push_back((int)shl.size() - out.sh_off.back());
+    // this chunk's shells grouped by l (stable), each keeping its compact
+    // AOs: only the launch order changes, not the layout of Phi
+    {
+      const int j0 = out.sh_off.back(), j1 = (int)shl.size();
+      std::vector<std::pair<int, int>> seg;
+      int cnt[kXcMaxL + 1] = {};
+      for (int j = j0; j < j1; ++j) {
+        const int l = std::min<int>(sh.l[shl[j]], kXcMaxL);
+        seg.push_back({shl[j], out0c[j]});
+        ++cnt[l];
+      }
+      int pos = j0;
+      for (int l = 0; l <= kXcMaxL; ++l) {
+        for (const auto& e : seg)
+          if (std::min<int>(sh.l[e.first], kXcMaxL) == l) {
+            shl[pos] = e.first;
+            out0c[pos] = e.second;
+            ++pos;
+          }
+        out.sh_lcnt.push_back(cnt[l]);
+      }
+    }
     out.ao_cnt.push_back(nao_c);
     out.max_ao = std::max(out.max_ao, nao_c);
     out.total_ao += nao_c;
@@ -620,10 +639,26 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
       continue;
     }
     const int64_t plane = (int64_t)nsig * G;
-    ao_kernel<<<dim3((unsigned)((G + kAoThreads - 1) / kAoThreads), (unsigned)nsh), kAoThreads, 0,
-                bs>>>(ov, ch.d_sh.as<int>() + ch.sh_off[k], ch.d_sh_out0.as<int>() + ch.sh_off[k],
-                      pts, g0, ng, G, nsig, b.phi.as<double>(), b.dphi.as<double>());
-    DFJK_LAUNCHED();
+    // the chunk's shells are grouped by l: one launch per l present
+    int j0 = ch.sh_off[k];
+    for (int l = 0; l < kXcMaxL + 1; ++l) {
+      const int cnt = ch.sh_lcnt[(size_t)k * (kXcMaxL + 1) + l];
+      if (cnt == 0) continue;
+      const dim3 grid((unsigned)((G + kAoThreads - 1) / kAoThreads), (unsigned)cnt);
+      const int* shl = ch.d_sh.as<int>() + j0;
+      const int* o0 = ch.d_sh_out0.as<int>() + j0;
+      double* ph = b.phi.as<double>();
+      double* dph = b.dphi.as<double>();
+      switch (l) {
+        case 0: ao_kernel<0><<<grid, kAoThreads, 0, bs>>>(ov, shl, o0, pts, g0, ng, G, nsig, ph, dph); break;
+        case 1: ao_kernel<1><<<grid, kAoThreads, 0, bs>>>(ov, shl, o0, pts, g0, ng, G, nsig, ph, dph); break;
+        case 2: ao_kernel<2><<<grid, kAoThreads, 0, bs>>>(ov, shl, o0, pts, g0, ng, G, nsig, ph, dph); break;
+        default: ao_kernel<3><<<grid, kAoThreads, 0, bs>>>(ov, shl, o0, pts, g0, ng, G, nsig, ph, dph); break;
+      }
+      DFJK_LAUNCHED();
+      j0 += cnt;
+    }
+    (void)nsh;
     gather_p_kernel<<<(unsigned)(((int64_t)nsig * nsig + 255) / 256), 256, 0, bs>>>(
         P, nao, map, nsig, b.Pc.as<double>());
     DFJK_LAUNCHED();
