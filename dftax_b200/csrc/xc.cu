@@ -204,24 +204,40 @@ __global__ void scatter_v_kernel(const double* __restrict__ Vc, int nsig, const 
 // consecutive points of two mu rows), so an 8192-point chunk fills 512
 // blocks; the 16 partial sums are added in a fixed order, so the result does
 // not depend on the launch.
-constexpr int kRhoPts = 16, kRhoLanes = 16;
-__global__ void __launch_bounds__(kRhoPts * kRhoLanes) rho_kernel(
+// rho and grad rho of 2 kRhoPairs points per block: each thread takes two
+// neighbouring points (16-byte loads; G is a multiple of 256, so the pair
+// stays inside the chunk, and the padding points hold zeros) and every
+// kRhoLanes-th function from ml, two functions per step; the kRhoLanes
+// partial sums are added in a fixed order
+constexpr int kRhoPairs = 16, kRhoLanes = 16;
+__global__ void __launch_bounds__(kRhoPairs * kRhoLanes) rho_kernel(
     const double* __restrict__ X, const double* __restrict__ phi, const double* __restrict__ dphi,
     int nao, int64_t G, int64_t ng, double* __restrict__ rho, double* __restrict__ grad) {
-  __shared__ double red[4][kRhoLanes][kRhoPts];
-  const int gi = threadIdx.x % kRhoPts, ml = threadIdx.x / kRhoPts;
-  const int64_t g = blockIdx.x * (int64_t)kRhoPts + gi;
+  __shared__ double2 red[4][kRhoLanes][kRhoPairs];
+  const int gi = threadIdx.x % kRhoPairs, ml = threadIdx.x / kRhoPairs;
+  const int64_t g = 2 * (blockIdx.x * (int64_t)kRhoPairs + gi);
   const int64_t plane = (int64_t)nao * G;
-  double r = 0.0, a = 0.0, b = 0.0, c = 0.0;
+  double2 r = {0.0, 0.0}, a = {0.0, 0.0}, b = {0.0, 0.0}, c = {0.0, 0.0};
+  auto ld2 = [](const double* p) { return *reinterpret_cast<const double2*>(p); };
+  auto acc = [&](int64_t o) {
+    const double2 x = ld2(X + o), f = ld2(phi + o), dx = ld2(dphi + o),
+                  dy = ld2(dphi + plane + o), dz = ld2(dphi + 2 * plane + o);
+    r.x += x.x * f.x;
+    r.y += x.y * f.y;
+    a.x += x.x * dx.x;
+    a.y += x.y * dx.y;
+    b.x += x.x * dy.x;
+    b.y += x.y * dy.y;
+    c.x += x.x * dz.x;
+    c.y += x.y * dz.y;
+  };
   if (g < ng) {
-    for (int mu = ml; mu < nao; mu += kRhoLanes) {
-      const int64_t o = (int64_t)mu * G + g;
-      const double x = X[o];
-      r += x * phi[o];
-      a += x * dphi[o];
-      b += x * dphi[plane + o];
-      c += x * dphi[2 * plane + o];
+    int mu = ml;
+    for (; mu + kRhoLanes < nao; mu += 2 * kRhoLanes) {
+      acc((int64_t)mu * G + g);
+      acc((int64_t)(mu + kRhoLanes) * G + g);
     }
+    if (mu < nao) acc((int64_t)mu * G + g);
   }
   red[0][ml][gi] = r;
   red[1][ml][gi] = a;
@@ -229,11 +245,16 @@ __global__ void __launch_bounds__(kRhoPts * kRhoLanes) rho_kernel(
   red[3][ml][gi] = c;
   __syncthreads();
   if (ml < 4 && g < ng) {
-    double t = 0.0;
+    double2 t = {0.0, 0.0};
 #pragma unroll
-    for (int q = 0; q < kRhoLanes; ++q) t += red[ml][q][gi];
-    if (ml == 0) rho[g] = t;
-    else grad[(ml - 1) * G + g] = 2.0 * t;
+    for (int q = 0; q < kRhoLanes; ++q) {
+      t.x += red[ml][q][gi].x;
+      t.y += red[ml][q][gi].y;
+    }
+    const double f = ml == 0 ? 1.0 : 2.0;
+    double* out = ml == 0 ? rho : grad + (ml - 1) * G;
+    out[g] = f * t.x;
+    if (g + 1 < ng) out[g + 1] = f * t.y;
   }
 }
 
@@ -666,7 +687,7 @@ static void xc_enqueue(const Context& c, const OrbView& ov, const double* pts, c
     DFJK_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)G, nsig, nsig, &one,
                             b.phi.as<double>(), (int)G, b.Pc.as<double>(), nsig, &zero,
                             b.X.as<double>(), (int)G));
-    rho_kernel<<<(unsigned)((ng + kRhoPts - 1) / kRhoPts), kRhoPts * kRhoLanes, 0, bs>>>(
+    rho_kernel<<<(unsigned)((ng + 2 * kRhoPairs - 1) / (2 * kRhoPairs)), kRhoPairs * kRhoLanes, 0, bs>>>(
         b.X.as<double>(), b.phi.as<double>(), b.dphi.as<double>(), nsig, G, ng,
         b.vr.as<double>(), b.vg.as<double>());
     DFJK_LAUNCHED();
