@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <utility>
 
 namespace dfjk {
@@ -479,50 +480,87 @@ static uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
   return spread(x) | spread(y) << 1 | spread(z) << 2;
 }
 
+// runs fn(t) for t = 0 .. T-1 on T host threads (the caller runs t = 0)
+template <class F>
+static void on_threads(int T, F&& fn) {
+  std::vector<std::thread> th;
+  th.reserve(T > 1 ? T - 1 : 0);
+  for (int t = 1; t < T; ++t) th.emplace_back([&fn, t] { fn(t); });
+  fn(0);
+  for (auto& x : th) x.join();
+}
+
 void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
   const int64_t n = (int64_t)w.size();
   if (n == 0) return;
+  // contiguous index ranges, one per host thread (one thread below 64 k points)
+  const int T = n < ((int64_t)1 << 16)
+                    ? 1
+                    : (int)std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()));
+  auto lo_of = [&](int t) { return n * t / T; };
   // Morton order of 1-Bohr cells
+  std::vector<double> los((size_t)3 * T, INFINITY);
+  on_threads(T, [&](int t) {
+    for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i)
+      for (int d = 0; d < 3; ++d) los[3 * t + d] = std::min(los[3 * t + d], pts[3 * i + d]);
+  });
   double lo[3] = {INFINITY, INFINITY, INFINITY};
-  for (int64_t i = 0; i < n; ++i)
-    for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], pts[3 * i + d]);
-  std::vector<uint64_t> code(n);
-  uint64_t cmax = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    uint64_t c[3];
-    for (int d = 0; d < 3; ++d) c[d] = (uint64_t)std::floor(pts[3 * i + d] - lo[d]);
-    code[i] = morton3(c[0], c[1], c[2]);
-    cmax = std::max(cmax, code[i]);
-  }
-  // order by (code, index): a stable LSD radix sort of the codes, 11 bits
-  // a pass over the bits cmax needs (the outermost radial points lie
-  // thousands of Bohr out, so the codes span tens of bits)
+  for (int t = 0; t < T; ++t)
+    for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], los[3 * t + d]);
+  std::vector<uint64_t> code(n), ktmp(n), cmaxs(T, 0);
+  std::vector<int64_t> order(n), otmp(n);
+  on_threads(T, [&](int t) {
+    for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) {
+      uint64_t c[3];
+      for (int d = 0; d < 3; ++d) c[d] = (uint64_t)std::floor(pts[3 * i + d] - lo[d]);
+      code[i] = morton3(c[0], c[1], c[2]);
+      cmaxs[t] = std::max(cmaxs[t], code[i]);
+      order[i] = i;
+    }
+  });
+  const uint64_t cmax = *std::max_element(cmaxs.begin(), cmaxs.end());
+  // order by (code, index): a stable LSD radix sort of the codes, 11 bits a
+  // pass over the bits cmax needs. Per pass each thread counts its range;
+  // the offsets run bucket by bucket and, within a bucket, thread by thread,
+  // so every thread's elements land after those of lower indices (stable)
   int bits = 0;
   while (bits < 64 && (cmax >> bits) != 0) ++bits;
   constexpr int kRadixBits = 11;
-  constexpr uint64_t kMask = ((uint64_t)1 << kRadixBits) - 1;
-  std::vector<int64_t> order(n), otmp(n);
-  std::vector<uint64_t> ktmp(n);
-  for (int64_t i = 0; i < n; ++i) order[i] = i;
-  std::vector<int64_t> cnt(kMask + 2);
+  constexpr uint64_t kBuckets = (uint64_t)1 << kRadixBits, kMask = kBuckets - 1;
+  std::vector<int64_t> hist((size_t)T * kBuckets);
   for (int shift = 0; shift < bits; shift += kRadixBits) {
-    std::fill(cnt.begin(), cnt.end(), 0);
-    for (int64_t i = 0; i < n; ++i) cnt[((code[i] >> shift) & kMask) + 1]++;
-    for (uint64_t k = 0; k <= kMask; ++k) cnt[k + 1] += cnt[k];
-    for (int64_t i = 0; i < n; ++i) {
-      const int64_t dst = cnt[(code[i] >> shift) & kMask]++;
-      ktmp[dst] = code[i];
-      otmp[dst] = order[i];
-    }
+    on_threads(T, [&](int t) {
+      int64_t* h = hist.data() + (size_t)t * kBuckets;
+      std::fill(h, h + kBuckets, 0);
+      for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) h[(code[i] >> shift) & kMask]++;
+    });
+    int64_t run = 0;
+    for (uint64_t b = 0; b < kBuckets; ++b)
+      for (int t = 0; t < T; ++t) {
+        int64_t& h = hist[(size_t)t * kBuckets + b];
+        const int64_t c = h;
+        h = run;
+        run += c;
+      }
+    on_threads(T, [&](int t) {
+      int64_t* h = hist.data() + (size_t)t * kBuckets;
+      for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) {
+        const int64_t dst = h[(code[i] >> shift) & kMask]++;
+        ktmp[dst] = code[i];
+        otmp[dst] = order[i];
+      }
+    });
     code.swap(ktmp);
     order.swap(otmp);
   }
   std::vector<double> p2(3 * n), w2(n);
-  for (int64_t i = 0; i < n; ++i) {
-    const int64_t j = order[i];
-    for (int d = 0; d < 3; ++d) p2[3 * i + d] = pts[3 * j + d];
-    w2[i] = w[j];
-  }
+  on_threads(T, [&](int t) {
+    for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) {
+      const int64_t j = order[i];
+      for (int d = 0; d < 3; ++d) p2[3 * i + d] = pts[3 * j + d];
+      w2[i] = w[j];
+    }
+  });
   pts.swap(p2);
   w.swap(w2);
 }
