@@ -60,6 +60,7 @@ struct dfscf {
   dfscf_result res{};
   bool have_orbitals = false;
   bool orbitals_current = false;   // C / eps diagonalize the Fock matrix of the last density
+  bool fx_valid = false;           // Fx holds the last run's final DIIS Fock matrix
   int64_t tuned_chunk = 0;   // XC points per chunk chosen by the autotuner (0: not tuned)
 };
 
@@ -540,6 +541,7 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
   const int n = f.nao, m = f.nmo, md = f.o.diis_space;
   const int64_t nn = (int64_t)n * n, mm = (int64_t)m * m;
   f.res = dfscf_result{};
+  f.fx_valid = false;
   f.res.nmo = f.nmo;
   f.res.nocc = f.nocc;
   bool orbitals;
@@ -596,6 +598,7 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
     }
     // the DIIS Fock moves to its own buffer before make_density reuses A1/A2
     DFJK_CUDA(cudaMemcpyAsync(f.Fx.p, Fext, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    f.fx_valid = true;
     tm.add(f.res.ms_diis);
     make_density(f, f.Fx.as<double>(), s);
     const double e = energy_fock(f, f.P.as<double>(), true, f.F.as<double>(), s);
@@ -603,9 +606,9 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
     e_prev = e;
     ++it;
   }
-  // orbitals and energies of the last DIIS Fock matrix when the density came
-  // from the projection (the density itself stays)
-  if (it > 0 && !f.orbitals_current) make_density_eig(f, f.Fx.as<double>(), s, false);
+  // when the last density came from the projection, the orbitals and
+  // energies of the last DIIS Fock matrix are computed by the first
+  // dfscf_get_orbitals (the batch engine, which reads only densities, skips it)
   f.res.e_tot = e_prev;
   f.res.derr = derr;
   f.res.xc_chunk = f.xcw.ch.G;
@@ -873,8 +876,16 @@ dfjk_status dfscf_get_density(dfscf* f, double* P, void* stream) {
 dfjk_status dfscf_get_orbitals(dfscf* f, double* eps, double* C, void* stream) {
   if (!f) return DFJK_ERR_INVALID;
   return guard(f->c, [&] {
-    if (!f->have_orbitals) fail(DFJK_ERR_STATE, "no orbitals before dfscf_run");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!f->orbitals_current && f->fx_valid) {
+      // the last density came from the projection: diagonalize that run's
+      // last DIIS Fock matrix now (the density stays; the run's timings too)
+      DFJK_CUDA(cudaSetDevice(f->c->device));
+      const double ms = f->res.ms_diag;
+      make_density_eig(*f, f->Fx.as<double>(), s, false);
+      f->res.ms_diag = ms;
+    }
+    if (!f->have_orbitals) fail(DFJK_ERR_STATE, "no orbitals before dfscf_run");
     if (eps)
       DFJK_CUDA(cudaMemcpyAsync(eps, f->eps.p, (size_t)f->nmo * sizeof(double),
                                 cudaMemcpyDeviceToDevice, s));

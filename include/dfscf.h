@@ -55,7 +55,9 @@ typedef struct {
                            aufbau density when the HOMO-LUMO gap is open, falling back
                            to the eigensolver for that iteration when the projection
                            does not converge (no gap). The orbitals and energies of
-                           dfscf_get_orbitals come from the eigensolver either way  */
+                           dfscf_get_orbitals come from the eigensolver either way
+                           (after a projected density, the first call computes them
+                           from the run's last DIIS Fock matrix)                     */
 } dfscf_options;
 
 typedef struct {
