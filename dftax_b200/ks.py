@@ -250,6 +250,8 @@ def _main(argv=None):
     ap.add_argument("--repeat", type=int, default=1, help="solves (the last one is reported)")
     ap.add_argument("--guess", default="core", choices=["core", "sad"])
     ap.add_argument("--density", default="purify", choices=sorted(DENSITY_ROUTES))
+    ap.add_argument("--xc-streams", type=int, default=0,
+                    help="concurrent streams of the XC chunks (0: 8; the batch engine uses 1)")
     ap.add_argument("--streamed", action="store_true",
                     help="streamed DF (B rebuilt per J/K call, not held): df(aux, chunk=...)")
     a = ap.parse_args(argv)
@@ -258,7 +260,7 @@ def _main(argv=None):
         t0 = time.perf_counter()
         ks = KS(sym, xyz, orb, coulomb=df(aux, precision=a.precision,
                                            chunk=1 if a.streamed else None), xc=a.xc,
-                grid=becke(a.radial, a.lebedev), density=a.density)
+                grid=becke(a.radial, a.lebedev), density=a.density, xc_streams=a.xc_streams)
         r = scf(ks, guess=a.guess)
         sec = time.perf_counter() - t0
         ks.close()
@@ -267,7 +269,8 @@ def _main(argv=None):
                       "guess": a.guess, "density": a.density, "streamed": a.streamed,
                       "e_tot": r.e_tot, "converged": r.converged, "n_iter": r.n_iter,
                       "seconds": round(sec, 3), "parts_ms": r.timings_ms,
-                      "xc_chunk": r.xc_chunk, "xc_graph": r.xc_graph, "n_eig": r.n_eig}))
+                      "xc_chunk": r.xc_chunk, "xc_graph": r.xc_graph, "n_eig": r.n_eig,
+                      "xc_gemm_tflop": round(r.xc_gemm_flop / 1e12, 4)}))
 
 
 if __name__ == "__main__":
