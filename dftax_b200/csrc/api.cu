@@ -376,13 +376,9 @@ static void parse_basis(const dfjk_basis* b, const char* what, int lmax_supporte
     const int nth = cells > (1 << 22)
                         ? (int)std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency()))
                         : 1;
-    {
-      std::vector<std::thread> th;
-      for (int t = 1; t < nth; ++t)
-        th.emplace_back(scan, (int)((int64_t)sh.n * t / nth), (int)((int64_t)sh.n * (t + 1) / nth));
-      scan(0, sh.n / nth);
-      for (auto& x : th) x.join();
-    }
+    run_on_threads(nth, [&](int t) {
+      scan((int)((int64_t)sh.n * t / nth), (int)((int64_t)sh.n * (t + 1) / nth));
+    });
     for (int s = 0; s < sh.n; ++s) {
       const int l = sh.l[s], nc = ncart(l), no = 2 * l + 1, r0 = sh.row0[s], c0 = sh.out0[s];
       const double rows = row_abs[s];
@@ -441,10 +437,7 @@ static void for_ranges(int nth, int64_t n, F f) {
     f(0, (int64_t)0, n);
     return;
   }
-  std::vector<std::thread> th;
-  for (int t = 1; t < nth; ++t) th.emplace_back(f, t, n * t / nth, n * (t + 1) / nth);
-  f(0, (int64_t)0, n / nth);
-  for (auto& x : th) x.join();
+  run_on_threads(nth, [&](int t) { f(t, n * t / nth, n * (t + 1) / nth); });
 }
 
 static void make_orbital_tables(Plan& p);

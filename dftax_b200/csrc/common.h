@@ -13,6 +13,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dfjk.h"
@@ -81,6 +82,34 @@ void cache_trim(int dev);            // cudaFree every cached buffer of dev
 // makes: those fail while any stream of the device is capturing, and the
 // batch engine's workers capture and allocate from different threads.
 std::recursive_mutex& capture_mutex();
+
+// Runs fn(t) for t = 0 .. T-1: t > 0 on host threads, t = 0 on the caller. A
+// thread that cannot be started runs on the caller instead; the first
+// exception any call throws is rethrown once every thread has joined.
+template <class F>
+void run_on_threads(int T, F&& fn) {
+  std::exception_ptr err;
+  std::mutex mu;
+  auto call = [&](int t) {
+    try {
+      fn(t);
+    } catch (...) {
+      std::lock_guard<std::mutex> lk(mu);
+      if (!err) err = std::current_exception();
+    }
+  };
+  std::vector<std::thread> th;
+  int started = 1;
+  try {
+    th.reserve(T > 1 ? T - 1 : 0);
+    for (; started < T; ++started) th.emplace_back(call, started);
+  } catch (...) {
+  }
+  for (int t = started; t < T; ++t) call(t);
+  call(0);
+  for (auto& x : th) x.join();
+  if (err) std::rethrow_exception(err);
+}
 
 // Device buffer owned by a plan or context (allocated through the cache).
 struct DevBuf {

@@ -480,16 +480,6 @@ static uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
   return spread(x) | spread(y) << 1 | spread(z) << 2;
 }
 
-// runs fn(t) for t = 0 .. T-1 on T host threads (the caller runs t = 0)
-template <class F>
-static void on_threads(int T, F&& fn) {
-  std::vector<std::thread> th;
-  th.reserve(T > 1 ? T - 1 : 0);
-  for (int t = 1; t < T; ++t) th.emplace_back([&fn, t] { fn(t); });
-  fn(0);
-  for (auto& x : th) x.join();
-}
-
 void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
   const int64_t n = (int64_t)w.size();
   if (n == 0) return;
@@ -500,7 +490,7 @@ void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
   auto lo_of = [&](int t) { return n * t / T; };
   // Morton order of 1-Bohr cells
   std::vector<double> los((size_t)3 * T, INFINITY);
-  on_threads(T, [&](int t) {
+  run_on_threads(T, [&](int t) {
     for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i)
       for (int d = 0; d < 3; ++d) los[3 * t + d] = std::min(los[3 * t + d], pts[3 * i + d]);
   });
@@ -509,7 +499,7 @@ void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
     for (int d = 0; d < 3; ++d) lo[d] = std::min(lo[d], los[3 * t + d]);
   std::vector<uint64_t> code(n), ktmp(n), cmaxs(T, 0);
   std::vector<int64_t> order(n), otmp(n);
-  on_threads(T, [&](int t) {
+  run_on_threads(T, [&](int t) {
     for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) {
       uint64_t c[3];
       for (int d = 0; d < 3; ++d) c[d] = (uint64_t)std::floor(pts[3 * i + d] - lo[d]);
@@ -529,7 +519,7 @@ void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
   constexpr uint64_t kBuckets = (uint64_t)1 << kRadixBits, kMask = kBuckets - 1;
   std::vector<int64_t> hist((size_t)T * kBuckets);
   for (int shift = 0; shift < bits; shift += kRadixBits) {
-    on_threads(T, [&](int t) {
+    run_on_threads(T, [&](int t) {
       int64_t* h = hist.data() + (size_t)t * kBuckets;
       std::fill(h, h + kBuckets, 0);
       for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) h[(code[i] >> shift) & kMask]++;
@@ -542,7 +532,7 @@ void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
         h = run;
         run += c;
       }
-    on_threads(T, [&](int t) {
+    run_on_threads(T, [&](int t) {
       int64_t* h = hist.data() + (size_t)t * kBuckets;
       for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) {
         const int64_t dst = h[(code[i] >> shift) & kMask]++;
@@ -554,7 +544,7 @@ void xc_sort(std::vector<double>& pts, std::vector<double>& w) {
     order.swap(otmp);
   }
   std::vector<double> p2(3 * n), w2(n);
-  on_threads(T, [&](int t) {
+  run_on_threads(T, [&](int t) {
     for (int64_t i = lo_of(t); i < lo_of(t + 1); ++i) {
       const int64_t j = order[i];
       for (int d = 0; d < 3; ++d) p2[3 * i + d] = pts[3 * j + d];
