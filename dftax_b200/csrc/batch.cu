@@ -264,7 +264,19 @@ dfjk_status dfbatch_create(int device, const dfbatch_options* opts, dfbatch** ou
     DFJK_CUDA(cudaMemGetInfo(&free_b, &total_b));
     e->budget = e->o.hbm_budget > 0 ? e->o.hbm_budget : (int64_t)(0.85 * (double)free_b);
     e->t0 = clock_type::now();
-    for (int w = 0; w < e->o.workers; ++w) e->workers.emplace_back(worker_main, e.get(), w);
+    try {
+      for (int w = 0; w < e->o.workers; ++w) e->workers.emplace_back(worker_main, e.get(), w);
+    } catch (...) {
+      // a worker that cannot be started: stop and join those that were
+      {
+        std::lock_guard<std::mutex> lk(e->mu);
+        e->stop = true;
+      }
+      e->cv_work.notify_all();
+      for (auto& t : e->workers) t.join();
+      e->workers.clear();
+      throw;
+    }
   });
   if (st != DFJK_OK) return st;
   *out = e.release();
