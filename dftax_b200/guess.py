@@ -118,10 +118,10 @@ def config_occupations(C, S, ao_l, Z) -> np.ndarray:
 
 def _shells(b: BasisData):
     """(first cartesian row, l) of every shell, in order."""
-    ang = np.asarray(b.angular)
+    lrow = np.asarray(b.angular).sum(axis=1)
     out, i = [], 0
-    while i < ang.shape[0]:
-        l = int(ang[i].sum())
+    while i < lrow.shape[0]:
+        l = int(lrow[i])
         out.append((i, l))
         i += (l + 1) * (l + 2) // 2
     return out
@@ -133,22 +133,29 @@ def atom_blocks(b: BasisData, atom_xyz, tol: float = 1e-10):
     cen = np.asarray(b.centers, dtype=np.float64)
     xyz = np.asarray(atom_xyz, dtype=np.float64).reshape(-1, 3)
     sph = b.cart2sph is not None
-    owner, c0, f0 = [], [0], [0]
-    for start, l in _shells(b):
-        d = np.linalg.norm(xyz - cen[start], axis=1)
-        a = int(np.argmin(d))
-        if d[a] > tol:
-            raise ValueError("a shell center is on no atom")
-        owner.append(a)
-        c0.append(c0[-1] + (l + 1) * (l + 2) // 2)
-        f0.append(f0[-1] + (2 * l + 1 if sph else (l + 1) * (l + 2) // 2))
-    out = []
-    for a in range(len(xyz)):
-        ks = [k for k, o in enumerate(owner) if o == a]
-        if not ks or ks != list(range(ks[0], ks[0] + len(ks))):
-            raise ValueError(f"atom {a}: no shells, or shells not contiguous")
-        out.append((slice(c0[ks[0]], c0[ks[-1] + 1]), slice(f0[ks[0]], f0[ks[-1] + 1])))
-    return out
+    sh = _shells(b)
+    start = np.array([st for st, _ in sh], dtype=np.int64)
+    ls = np.array([l for _, l in sh], dtype=np.int64)
+    # nearest atom of each shell center (the first of equals, as argmin)
+    d = np.linalg.norm(cen[start][:, None, :] - xyz[None, :, :], axis=2)
+    owner = d.argmin(axis=1)
+    if (d[np.arange(len(sh)), owner] > tol).any():
+        raise ValueError("a shell center is on no atom")
+    ncart = (ls + 1) * (ls + 2) // 2
+    c0 = np.concatenate([[0], np.cumsum(ncart)])
+    f0 = np.concatenate([[0], np.cumsum(2 * ls + 1 if sph else ncart)])
+    # each atom's first and last shell; contiguous when they span its count
+    na, idx = len(xyz), np.arange(len(sh))
+    cnt = np.bincount(owner, minlength=na)
+    first = np.full(na, len(sh))
+    last = np.full(na, -1)
+    np.minimum.at(first, owner, idx)
+    np.maximum.at(last, owner, idx)
+    bad = np.nonzero((cnt == 0) | (last - first + 1 != cnt))[0]
+    if len(bad):
+        raise ValueError(f"atom {int(bad[0])}: no shells, or shells not contiguous")
+    return [(slice(int(c0[first[a]]), int(c0[last[a] + 1])),
+             slice(int(f0[first[a]]), int(f0[last[a] + 1]))) for a in range(na)]
 
 
 def _sub_basis(b: BasisData, cs: slice, fs: slice) -> BasisData:

@@ -154,3 +154,41 @@ def test_config_occupations_fill_channels_by_energy():
     C = np.eye(6)[:, [0, 3, 4, 5, 1, 2]]   # energy order: s, p, p, p, s, s
     occ = config_occupations(C, S, ao_l, 8)
     assert np.allclose(occ, [2, 4 / 3, 4 / 3, 4 / 3, 2, 0])
+
+
+def _atom_blocks_loop(b, xyz, tol=1e-10):
+    """The per-shell restatement: nearest atom of each shell center, then each
+    atom's contiguous run of shells."""
+    from dftax_b200.guess import _shells
+
+    cen = np.asarray(b.centers)
+    sph = b.cart2sph is not None
+    owner, c0, f0 = [], [0], [0]
+    for start, l in _shells(b):
+        d = np.linalg.norm(xyz - cen[start], axis=1)
+        a = int(np.argmin(d))
+        assert d[a] <= tol
+        owner.append(a)
+        c0.append(c0[-1] + (l + 1) * (l + 2) // 2)
+        f0.append(f0[-1] + (2 * l + 1 if sph else (l + 1) * (l + 2) // 2))
+    out = []
+    for a in range(len(xyz)):
+        ks = [k for k, o in enumerate(owner) if o == a]
+        out.append((slice(c0[ks[0]], c0[ks[-1] + 1]), slice(f0[ks[0]], f0[ks[-1] + 1])))
+    return out
+
+
+@pytest.mark.parametrize("name", ["water3", "alkane2"])
+def test_atom_blocks_match_the_per_shell_form(name):
+    """The SAD guess's atomic blocks (orbital and auxiliary, spherical and
+    cartesian) against the per-shell restatement, and its two errors."""
+    from dftax_b200 import systems
+    from dftax_b200.guess import atom_blocks
+
+    sym, xyz, orb, aux, _ = systems.workload(name, seed=0)
+    for b in (orb, aux, systems.basis_for(sym, xyz, spherical=False)[0]):
+        assert atom_blocks(b, xyz) == _atom_blocks_loop(b, np.asarray(xyz))
+    with pytest.raises(ValueError, match="on no atom"):
+        atom_blocks(orb, np.asarray(xyz) + 0.1)
+    with pytest.raises(ValueError, match="no shells"):
+        atom_blocks(orb, np.vstack([xyz, [[50.0, 50.0, 50.0]]]))
