@@ -125,16 +125,18 @@ def becke_grid(symbols, coords_bohr, spec: Becke | None = None, *, device: int =
     spec = spec or Becke()
     coords = np.asarray(coords_bohr, dtype=np.float64).reshape(-1, 3)
     Zs = [ATOMIC_NUMBER[s] for s in symbols]
-    pts, raw, owner = [], [], []
-    for a, Z in enumerate(Zs):
-        off, w = _atom_template(Z, spec.n_radial, spec.lebedev, spec.prune,
-                                None if spec.r_max is None else float(spec.r_max))
-        pts.append(coords[a] + off)
-        raw.append(w)
-        owner.append(np.full(len(w), a, dtype=np.int32))
-    pts = np.ascontiguousarray(np.concatenate(pts))
-    raw = np.ascontiguousarray(np.concatenate(raw))
-    owner = np.ascontiguousarray(np.concatenate(owner))
+    tmpl = [_atom_template(Z, spec.n_radial, spec.lebedev, spec.prune,
+                           None if spec.r_max is None else float(spec.r_max)) for Z in Zs]
+    counts = np.array([len(w) for _, w in tmpl], dtype=np.int64)
+    n = int(counts.sum())
+    pts = np.empty((n, 3))
+    raw = np.empty(n)
+    o = 0
+    for a, (off, w) in enumerate(tmpl):
+        np.add(off, coords[a], out=pts[o:o + len(w)])
+        raw[o:o + len(w)] = w
+        o += len(w)
+    owner = np.repeat(np.arange(len(Zs), dtype=np.int32), counts)
     ctx = Context.get(device)
     dev = f"cuda:{ctx.device}"
     dp = torch.as_tensor(pts, device=dev)
@@ -146,11 +148,11 @@ def becke_grid(symbols, coords_bohr, spec: Becke | None = None, *, device: int =
     _lib.check(ctx.lib.dfjk_becke_partition(ctx.h, dp.data_ptr(), do.data_ptr(), dr.data_ptr(),
                                             len(raw), len(Zs), coords.ctypes.data,
                                             bragg.ctypes.data, dw.data_ptr(), stream), ctx.h)
-    w = dw.cpu().numpy()
     if spec.cutoff is not None:
-        keep = np.abs(w) > spec.cutoff
-        pts, w = pts[keep], w[keep]
-    return np.ascontiguousarray(pts), np.ascontiguousarray(w)
+        # the points of negligible weight are dropped on the device
+        keep = dw.abs() > spec.cutoff
+        return dp[keep].cpu().numpy(), dw[keep].cpu().numpy()
+    return pts, dw.cpu().numpy()
 
 
 __all__ = ["Becke", "becke", "becke_grid", "lebedev", "bragg_radius", "BRAGG_BOHR"]
