@@ -91,3 +91,35 @@ def test_no_gap_falls_back_to_the_eigensolver():
     assert a.e_tot == b.e_tot
     assert np.array_equal(a.P, b.P)
     assert np.array_equal(a.mo_energy, b.mo_energy)
+
+
+def test_density_option_is_checked_and_xc_work_reported():
+    """dfscf_create refuses a density route other than 0 or 1 (INVALID), and
+    the result reports the XC DGEMM work of one evaluation (none for HF)."""
+    import ctypes
+    from ctypes import byref
+
+    import torch
+
+    from dftax_b200 import _lib, df, systems
+    from dftax_b200.coulomb import _stream_ptr
+    from dftax_b200.ks import KS, scf
+
+    sym, xyz, orb, aux, _ = systems.workload("water", seed=0)
+    ks = KS(sym, xyz, orb, coulomb=df(aux))
+    o = _lib.ScfOptions()
+    ctypes.memmove(byref(o), byref(ks._opts), ctypes.sizeof(o))
+    o.density = 5
+    h = ctypes.c_void_p()
+    st = ks.lib.dfscf_create(ks.plan.h, len(ks.charges), ks.coords.ctypes.data,
+                             ks.charges.ctypes.data, len(ks.grid_weights),
+                             ks.grid_coords.ctypes.data, ks.grid_weights.ctypes.data,
+                             ks.nocc[0], byref(o), byref(h), _stream_ptr(torch))
+    assert st == _lib.DFJK_ERR_INVALID
+    assert "density must be 0 or 1" in ks.ctx.last_error()
+    r = scf(ks)
+    assert r.converged and r.xc_gemm_flop > 0
+    ks.close()
+    hf = KS(sym, xyz, orb, coulomb=df(aux), xc="HF")
+    assert scf(hf).xc_gemm_flop == 0
+    hf.close()
