@@ -621,10 +621,11 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
 // Points per XC chunk, chosen by timing: the chunk size sets the shapes of the
 // two DGEMMs per chunk (G x nsig x nsig) and the launches per evaluation.
 // Candidates 2048, 4096, 8192 and 16384 points are timed on the core-guess
-// density (three evaluations each, the faster of the last two counted,
-// launched directly) for the first molecule of each (nao / 128, log2 points,
-// XC streams) bucket; the choice is kept for the process, so later molecules
-// of that size (solves in a batch included) use it without timing.
+// density (four evaluations each: a direct one, the graph capture, and two
+// graph replays, the faster replay counted) for the first molecule of each
+// (nao / 128, log2 points, XC streams) bucket; the choice is kept for the
+// process, so later molecules of that size (solves in a batch included) use it
+// without timing.
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int>, int64_t>& tuned() {
   static auto* m = new std::map<std::tuple<int, int, int>, int64_t>();
@@ -645,12 +646,14 @@ void autotune_chunk(dfscf& f, const int (&nout)[8], const std::vector<double>& p
   if (best == 0) {
     make_density_eig(f, f.H.as<double>(), s);   // core-guess density to time on
     double best_ms = INFINITY;
-    f.xcw.graph_off = true;
     for (int64_t G : {2048, 4096, 8192, 16384}) {
       if ((int64_t)6 * f.nao * G * 8 > ((int64_t)3 << 30)) continue;
+      // as the SCF runs it: the first call launches directly, the second
+      // captures the CUDA graph, the timed ones replay it
       xc_chunk(f.p->orb, nout, pv, G, f.o.ao_thresh, f.xcw);
-      xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),
-                     f.Vxc.as<double>(), xc_params(f), f.xcw, s);
+      for (int rep = 0; rep < 2; ++rep)
+        xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),
+                       f.Vxc.as<double>(), xc_params(f), f.xcw, s);
       double ms = INFINITY;
       for (int rep = 0; rep < 2; ++rep) {
         const auto t0 = std::chrono::steady_clock::now();
@@ -664,7 +667,6 @@ void autotune_chunk(dfscf& f, const int (&nout)[8], const std::vector<double>& p
         best = G;
       }
     }
-    f.xcw.graph_off = false;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tuned().emplace(key, best);
   }
