@@ -621,11 +621,10 @@ void run(dfscf& f, const double* P0, cudaStream_t s) {
 // Points per XC chunk, chosen by timing: the chunk size sets the shapes of the
 // two DGEMMs per chunk (G x nsig x nsig) and the launches per evaluation.
 // Candidates 2048, 4096, 8192 and 16384 points are timed on the core-guess
-// density (four evaluations each: a direct one, the graph capture, and two
-// graph replays, the faster replay counted) for the first molecule of each
-// (nao / 128, log2 points, XC streams) bucket; the choice is kept for the
-// process, so later molecules of that size (solves in a batch included) use it
-// without timing.
+// density (three evaluations each: a direct one, the graph capture, and a
+// timed graph replay) for the first molecule of each (nao / 128, log2 points,
+// XC streams) bucket; the choice is kept for the process, so later molecules
+// of that size (solves in a batch included) use it without timing.
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int>, int64_t>& tuned() {
   static auto* m = new std::map<std::tuple<int, int, int>, int64_t>();
@@ -654,14 +653,11 @@ void autotune_chunk(dfscf& f, const int (&nout)[8], const std::vector<double>& p
       for (int rep = 0; rep < 2; ++rep)
         xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),
                        f.Vxc.as<double>(), xc_params(f), f.xcw, s);
-      double ms = INFINITY;
-      for (int rep = 0; rep < 2; ++rep) {
-        const auto t0 = std::chrono::steady_clock::now();
-        xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),
-                       f.Vxc.as<double>(), xc_params(f), f.xcw, s);
-        ms = std::min(ms, std::chrono::duration<double, std::milli>(
-                              std::chrono::steady_clock::now() - t0).count());
-      }
+      const auto t0 = std::chrono::steady_clock::now();
+      xc_energy_fock(*f.c, f.ov, f.pts.as<double>(), f.wts.as<double>(), f.P.as<double>(),
+                     f.Vxc.as<double>(), xc_params(f), f.xcw, s);
+      const double ms =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
       if (ms < best_ms) {
         best_ms = ms;
         best = G;
